@@ -1,0 +1,505 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 minfft engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference] [--workload NAME]
+
+Default workload ("2d2048"): 2-D real DFT + inverse real DFT and 2-D
+DCT-2 -> DCT-3 round trips on 2048 x 2048 arrays of i.i.d. standard-normal
+data, in double and in single precision.  One step = those 8 transforms
+(realdft, invrealdft, dct2, dct3 in f64, then in f32), each through the
+engine's C ABI on device-resident data.  Metric: GFLOP/s with the
+2.5 * N * log2(N) convention for real-data transforms (N = 2^22 points).
+
+Other workloads (``--workload``): "batch4096" (1024 complex DFTs of length
+4096, c128, forward then inverse; 5 N log2 N per transform).
+
+Timing: W untimed warm-up steps, then exactly K steps between CUDA events on
+the stream the kernels run on (the legacy default stream), bracketed by a
+barrier and a device synchronisation; the maximum over ranks is reported.
+Inputs rotate over 4 buffer sets, so each step reads inputs last touched
+four steps earlier, with far more than the 126 MB L2 written in between.
+
+Under torchrun every rank runs its own replica of the workload on its own
+GPU (the transforms are independent; there is no data-path collective):
+value = all ranks' FLOPs / max-over-ranks time, scaling "weak".
+
+``--impl reference`` times the reference's own CPU library (aimukhin/minfft
+compiled from its sources into oracle/_ref/, or the oracle restatement if it
+was not built) on the host cores: every OpenMP thread runs one independent
+instance of the same step with its own plans (a minfft plan is not
+re-entrant).  Only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_PATH = os.path.join(ROOT, "profiles", "traffic.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ------------------------------------------------------------------ helpers
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- workloads
+class Workload2D:
+    """2048 x 2048 realdft/invrealdft and dct2/dct3 round trips, f64 and f32."""
+
+    name = "2d2048"
+    dims = (2048, 2048)
+    nsets = 4
+
+    def __init__(self, torch, dev):
+        import minfft_b200
+
+        self.torch = torch
+        n = int(np.prod(self.dims))
+        self.flops_per_transform = 2.5 * n * math.log2(n)
+        self.ops_per_step = 8
+        rng = np.random.default_rng(2)
+        self.precs = []
+        for single in (False, True):
+            eng = minfft_b200.engine(single)
+            rdt = torch.float32 if single else torch.float64
+            cdt = torch.complex64 if single else torch.complex128
+            spec = (self.dims[0], self.dims[1] // 2 + 1)
+            xs = [torch.from_numpy(rng.standard_normal(self.dims)).to(dev, rdt) for _ in range(self.nsets)]
+            z = torch.empty(spec, dtype=cdt, device=dev)
+            x2 = torch.empty(self.dims, dtype=rdt, device=dev)
+            c = torch.empty(self.dims, dtype=rdt, device=dev)
+            x3 = torch.empty(self.dims, dtype=rdt, device=dev)
+            pr = eng.plan("realdft", self.dims)
+            pt = eng.plan("t2t3", self.dims)
+            self.precs.append(dict(single=single, eng=eng, pr=pr, pt=pt, xs=xs, z=z, x2=x2, c=c, x3=x3))
+
+    def plans(self):
+        for p in self.precs:
+            yield p["eng"], p["pr"], ("realdft", "invrealdft")
+            yield p["eng"], p["pt"], ("dct2", "dct3")
+
+    def step(self, k: int):
+        s = k % self.nsets
+        for p in self.precs:
+            x = p["xs"][s].data_ptr()
+            pr, pt = p["pr"], p["pt"]
+            pr("realdft", x, p["z"].data_ptr(), check=False)
+            pr("invrealdft", p["z"].data_ptr(), p["x2"].data_ptr(), check=False)
+            pt("dct2", x, p["c"].data_ptr(), check=False)
+            pt("dct3", p["c"].data_ptr(), p["x3"].data_ptr(), check=False)
+
+    def check_errors(self):
+        for p in self.precs:
+            p["eng"].check()
+
+    def launches_per_step(self):
+        tot = 0
+        for eng, plan, ops in self.plans():
+            tot += sum(eng.launch_count(op, plan.aux) for op in ops)
+        return tot
+
+    def e2e_setup(self):
+        """Pinned host copies of one input set and host outputs."""
+        torch = self.torch
+        self.host = []
+        for p in self.precs:
+            pin = lambda t: torch.empty(t.shape, dtype=t.dtype, pin_memory=True)  # noqa: E731
+            hx = pin(p["xs"][0])
+            hx.copy_(p["xs"][0].cpu())
+            self.host.append(dict(x=hx, z=pin(p["z"]), x2=pin(p["x2"]), c=pin(p["c"]), x3=pin(p["x3"])))
+        h2d = d2h = 0
+        for h in self.host:
+            # each call stages its input to the device and its output back
+            h2d += 2 * h["x"].numel() * h["x"].element_size() + h["z"].numel() * h["z"].element_size() + \
+                h["c"].numel() * h["c"].element_size()
+            d2h += h["z"].numel() * h["z"].element_size() + h["x2"].numel() * h["x2"].element_size() + \
+                h["c"].numel() * h["c"].element_size() + h["x3"].numel() * h["x3"].element_size()
+        return h2d, d2h
+
+    def e2e_step(self):
+        for p, h in zip(self.precs, self.host):
+            pr, pt = p["pr"], p["pt"]
+            pr("realdft", h["x"].data_ptr(), h["z"].data_ptr(), check=False)
+            pr("invrealdft", h["z"].data_ptr(), h["x2"].data_ptr(), check=False)
+            pt("dct2", h["x"].data_ptr(), h["c"].data_ptr(), check=False)
+            pt("dct3", h["c"].data_ptr(), h["x3"].data_ptr(), check=False)
+
+    def config(self):
+        return {"workload": "2-D realdft->invrealdft and dct2->dct3 round trips, 2048x2048, f64 and f32",
+                "dims": list(self.dims), "precisions": ["f64", "f32"], "transforms_per_step": 8,
+                "flops": "2.5*N*log2(N) per transform, N=2^22",
+                "inputs": "i.i.d. standard normal, numpy PCG64 seed 2",
+                "l2": "inputs rotate over 4 buffer sets (192 MiB of inputs; each step writes ~250 MB), "
+                      "larger than the 126 MB L2"}
+
+    # CPU reference: (family, ops, single) sequences of one step
+    cpu_sequences = (("realdft", ("realdft", "invrealdft"), False), ("t2t3", ("dct2", "dct3"), False),
+                     ("realdft", ("realdft", "invrealdft"), True), ("t2t3", ("dct2", "dct3"), True))
+
+
+class WorkloadBatch4096:
+    """1024 independent complex DFTs of length 4096 (c128), forward then inverse."""
+
+    name = "batch4096"
+    n, howmany = 4096, 1024
+    nsets = 4
+
+    def __init__(self, torch, dev):
+        import minfft_b200
+
+        self.torch = torch
+        self.flops_per_transform = 5.0 * self.n * math.log2(self.n) * self.howmany
+        self.ops_per_step = 2
+        rng = np.random.default_rng(1)
+        shape = (self.howmany, self.n)
+        self.eng = minfft_b200.engine(False)
+        mk = lambda: torch.from_numpy(rng.uniform(-1, 1, shape) + 1j * rng.uniform(-1, 1, shape)).to(dev)  # noqa
+        self.xs = [mk() for _ in range(self.nsets)]
+        self.y = torch.empty(shape, dtype=torch.complex128, device=dev)
+        self.z = torch.empty(shape, dtype=torch.complex128, device=dev)
+        self.plan = self.eng.plan("dft", (self.n,))
+
+    def plans(self):
+        yield self.eng, self.plan, ("dft", "invdft")
+
+    def step(self, k):
+        x = self.xs[k % self.nsets]
+        self.plan.batch("dft", x.data_ptr(), self.y.data_ptr(), self.howmany)
+        self.plan.batch("invdft", self.y.data_ptr(), self.z.data_ptr(), self.howmany)
+
+    def check_errors(self):
+        self.eng.check()
+
+    def launches_per_step(self):
+        return 2
+
+    def e2e_setup(self):
+        t = self.torch
+        self.hx = t.empty(self.xs[0].shape, dtype=t.complex128, pin_memory=True)
+        self.hx.copy_(self.xs[0].cpu())
+        self.hy = t.empty_like(self.hx, pin_memory=True)
+        self.hz = t.empty_like(self.hx, pin_memory=True)
+        b = self.hx.numel() * 16
+        return 2 * b, 2 * b
+
+    def e2e_step(self):
+        self.plan.batch("dft", self.hx.data_ptr(), self.hy.data_ptr(), self.howmany)
+        self.plan.batch("invdft", self.hy.data_ptr(), self.hz.data_ptr(), self.howmany)
+
+    def config(self):
+        return {"workload": "1024 x complex DFT N=4096 c128, forward then inverse", "n": self.n,
+                "batch": self.howmany, "flops": "5*N*log2(N) per transform",
+                "inputs": "re/im i.i.d. uniform[-1,1), seed 1",
+                "l2": "inputs rotate over 4 sets of 64 MiB (256 MiB), larger than L2"}
+
+    cpu_sequences = None
+
+
+WORKLOADS = {"2d2048": Workload2D, "batch4096": WorkloadBatch4096}
+
+
+# -------------------------------------------------------------- CPU timing
+def cpu_run(kind: str, sequences, dims, batch: int, threads: int, reps: int, warm: int = 1, seed: int = 1):
+    """Seconds for `reps` timed sweeps (after `warm` untimed ones) of `batch`
+    independent instances of every (family, ops) sequence, on `threads`
+    OpenMP threads."""
+    import ctypes
+
+    import oracle
+
+    oracle.build()
+    cb = ctypes.CDLL(oracle.CPUBENCH_PATH)
+    cb.cpubench_run.restype = ctypes.c_double
+    cb.cpubench_run.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint]
+    fam_code = {"dft": 0, "realdft": 1, "t2t3": 2, "t4": 3}
+    op_code = {op: i for i, op in enumerate(("dft", "invdft", "realdft", "invrealdft", "dct2", "dst2", "dct3",
+                                             "dst3", "dct4", "dst4"))}
+    total = 0.0
+    for fam, ops, single in sequences:
+        path = oracle._PATHS[(kind, single)]
+        arr_ops = (ctypes.c_int * len(ops))(*[op_code[o] for o in ops])
+        arr_dims = (ctypes.c_int * len(dims))(*dims)
+        t = cb.cpubench_run(path.encode(), int(single), fam_code[fam], len(ops), arr_ops, len(dims), arr_dims,
+                            batch, threads, warm, reps, seed)
+        if t < 0:
+            raise RuntimeError(f"cpubench failed ({t}) for {fam} {ops}")
+        total += t
+    return total
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_kind():
+    import oracle
+
+    return oracle.best_kind()
+
+
+# ------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return 0
+    W = WORKLOADS[args.workload]
+    if W.cpu_sequences is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"no CPU sequence defined for workload {W.name}"}))
+        return 0
+    kind = cpu_kind()
+    P = cpu_threads()
+    n = int(np.prod(W.dims))
+    flops_step = 2.5 * n * math.log2(n) * 8
+    t = cpu_run(kind, W.cpu_sequences, W.dims, P, P, reps=args.steps, warm=args.warmup)
+    value = flops_step * P * args.steps / t / 1e9
+    line = {"metric": "GFLOP/s (5N log2N complex, 2.5N log2N real-data)", "value": round(value, 3),
+            "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1000 * t / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+            "config": _ref_config(W), "impl": "reference",
+            "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": P, "kind": kind,
+                             "sample": f"{P} concurrent independent instances of the step (one per thread, "
+                                       f"own plans), per timed step"},
+            "e2e": {"value": round(value, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def _ref_config(W):
+    cfg = {"workload": "2-D realdft->invrealdft and dct2->dct3 round trips, 2048x2048, f64 and f32",
+           "dims": list(W.dims), "precisions": ["f64", "f32"], "transforms_per_step": 8,
+           "flops": "2.5*N*log2(N) per transform, N=2^22"}
+    return cfg
+
+
+# ---------------------------------------------------------------- engine arm
+def run_engine(args):
+    import torch
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    W = WORKLOADS[args.workload](torch, dev)
+    launches_per_step = W.launches_per_step()
+
+    # warm-up
+    for k in range(args.warmup):
+        W.step(k)
+    torch.cuda.synchronize()
+    W.check_errors()
+
+    # launch-level timing on during the timed region (events between launches)
+    for eng, plan, ops in W.plans():
+        eng.profile(plan.aux, args.steps * 8 + 64)
+
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record()
+        for k in range(args.steps):
+            W.step(k)
+        end.record()
+        end.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    W.check_errors()
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    flops_step = W.flops_per_transform * W.ops_per_step
+    value = flops_step * args.steps * world / (ms / 1e3) / 1e9
+
+    # per-kernel statistics -> roofline of the dominant kernel
+    stats = []
+    for eng, plan, ops in W.plans():
+        prec = "f32" if eng.single else "f64"
+        for lab, cnt, tot, by in eng.profile_stats(plan.aux):
+            stats.append((f"{prec} {lab}", cnt, tot, by))
+        eng.profile(plan.aux, 0)
+    stats.sort(key=lambda r: -r[2])
+    hbm, peak_src = peaks()
+    roof = None
+    if stats:
+        lab, cnt, tot, by = stats[0]
+        avg_ms = tot / cnt
+        achieved = by / (avg_ms / 1e3) / 1e9
+        traffic = None
+        try:
+            with open(TRAFFIC_PATH) as f:
+                traffic = json.load(f).get(args.workload, {}).get(lab)
+        except Exception:
+            traffic = None
+        roof = {"bound": "hbm", "kernel": lab, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": by, "avg_launch_us": round(avg_ms * 1e3, 2),
+                "traffic": traffic}
+    kernel_table = [{"kernel": lab, "launches": cnt, "total_ms": round(tot, 3),
+                     "share": round(tot / sum(s[2] for s in stats), 4),
+                     "gbs": round(by / (tot / cnt / 1e3) / 1e9, 1)} for lab, cnt, tot, by in stats]
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        h2d, d2h = W.e2e_setup()
+        W.e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        W.e2e_step()
+        est = time.perf_counter() - t0
+        k_e2e = max(3, min(args.steps, int(5.0 / max(est, 1e-4))))
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            W.e2e_step()
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([el], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        W.check_errors()
+        e2e = {"value": round(flops_step * k_e2e * world / el / 1e9, 3), "unit": "GFLOP/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": k_e2e,
+               "ms_per_step": round(1000 * el / k_e2e, 3)}
+
+    # CPU baseline (rank 0, one GPU only): the reference on the host cores
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu and W.cpu_sequences is not None:
+        P = cpu_threads()
+        kind = cpu_kind()
+        t = cpu_run(kind, W.cpu_sequences, W.dims, P, P, 1)
+        cpu = {"value": round(flops_step * P / t / 1e9, 3), "unit": "GFLOP/s", "cores": P, "kind": kind,
+               "sample": f"{P} concurrent independent instances of one step (one per OpenMP thread, own plans), "
+                         f"{t:.1f} s"}
+
+    if rank == 0:
+        line = {"metric": "GFLOP/s (5N log2N complex, 2.5N log2N real-data)", "value": round(value, 3),
+                "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64+f32" if args.workload == "2d2048" else "f64",
+                "data": "synthetic", "config": W.config(), "parallelism": f"replicas x{world}",
+                "gpu_launches": int(launches_per_step * args.steps), "clocks": clocks.summary(),
+                "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "kernels": kernel_table[:8]}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="2d2048")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_engine(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

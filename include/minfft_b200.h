@@ -1,0 +1,94 @@
+/*
+ * minfft_b200.h -- extensions of the B200 transform engine beyond the
+ * reference API in minfft.h.  The reference library (aimukhin/minfft) has no
+ * counterpart for anything declared here: it is single-threaded, synchronous,
+ * returns no error codes and has no batch interface.
+ *
+ * Conventions: functions returning int return 0 on success or a
+ * MINFFT_B200_E* code; the code of the last failure on the calling thread is
+ * also kept for minfft_b200_last_error().  Pointers named "stream" are
+ * cudaStream_t values.
+ */
+#ifndef MINFFT_B200_H
+#define MINFFT_B200_H
+
+#include "minfft.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- errors */
+enum {
+    MINFFT_B200_OK = 0,
+    MINFFT_B200_EINVAL = 1,      /* bad argument: NULL plan, wrong plan kind, bad size */
+    MINFFT_B200_ENOMEM = 2,      /* device or host allocation failed */
+    MINFFT_B200_ECUDA = 3,       /* a CUDA runtime call failed */
+    MINFFT_B200_EUNSUPPORTED = 4,/* valid request this build cannot run */
+    MINFFT_B200_ETIMEOUT = 5     /* a bounded device-side wait gave up */
+};
+
+/* Code of the most recent failure on this thread (0 if none) and clear it.
+ * minfft.h's transforms return void, so this is how a caller learns that a
+ * call was rejected (e.g. invdft given a t4 plan) or that CUDA failed. */
+int minfft_b200_last_error(void);
+/* Text of the most recent failure on this thread ("" if none). */
+const char *minfft_b200_last_error_message(void);
+
+/* --------------------------------------------------------------- streams */
+/* Work on device pointers is enqueued on the plan's stream and returns
+ * without waiting; calls with host pointers stage through device memory and
+ * return when the result is in host memory.  The default stream is the
+ * legacy default stream (0). */
+int minfft_b200_set_stream(minfft_aux *a, void *stream);
+void *minfft_b200_get_stream(const minfft_aux *a);
+int minfft_b200_synchronize(const minfft_aux *a);
+
+/* ------------------------------------------------------------ transforms */
+/* Transform codes for the generic entry points below. */
+enum {
+    MINFFT_B200_DFT = 0,
+    MINFFT_B200_INVDFT = 1,
+    MINFFT_B200_REALDFT = 2,
+    MINFFT_B200_INVREALDFT = 3,
+    MINFFT_B200_DCT2 = 4,
+    MINFFT_B200_DST2 = 5,
+    MINFFT_B200_DCT3 = 6,
+    MINFFT_B200_DST3 = 7,
+    MINFFT_B200_DCT4 = 8,
+    MINFFT_B200_DST4 = 9
+};
+
+/* Run transform `op` on `howmany` arrays stored back to back, each shaped
+ * as the plan's dimensions (input and output strides are the sizes of one
+ * input / output array).  howmany = 1 is exactly the minfft.h call. */
+int minfft_b200_execute_batch(int op, void *x, void *y, int howmany, const minfft_aux *a);
+
+/* Bytes of one input / output array of `op` for plan `a` (-1 on error). */
+long long minfft_b200_input_bytes(int op, const minfft_aux *a);
+long long minfft_b200_output_bytes(int op, const minfft_aux *a);
+
+/* Device bytes held by the plan (tables and scratch). */
+long long minfft_b200_plan_bytes(const minfft_aux *a);
+
+/* Number of kernel launches one call of `op` enqueues (after planning). */
+int minfft_b200_launch_count(int op, const minfft_aux *a);
+
+/* ------------------------------------------------------ launch timing */
+/* With profiling enabled, every kernel launch of the plan's subsequent
+ * calls is bracketed by CUDA events on the plan's stream (no host
+ * synchronisation).  Reading the statistics synchronises and folds the
+ * recorded timings into one entry per kernel label: number of launches,
+ * total milliseconds and algorithmic bytes per launch (inputs read once,
+ * outputs written once).  Enabling (or disabling) clears the statistics;
+ * enable > 1 also pre-creates events for that many launches. */
+int minfft_b200_profile(minfft_aux *a, int enable);
+int minfft_b200_profile_count(minfft_aux *a);
+int minfft_b200_profile_entry(minfft_aux *a, int i, const char **label, long long *launches, double *total_ms,
+                              double *bytes_per_launch);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* MINFFT_B200_H */

@@ -1,0 +1,212 @@
+"""minfft_b200 -- a B200 (sm_100a) transform engine behind minfft's C API.
+
+The product is the pair of shared libraries built from ``csrc/`` by
+``python -m minfft_b200.build``:
+
+* ``lib/libminfft_b200.so``        -- double precision (minfft's default)
+* ``lib/libminfft_b200_single.so`` -- single precision (minfft's MINFFT_SINGLE)
+
+Both export the 27 symbols of ``include/minfft.h`` (identical to the
+reference minfft.h) plus the extensions of ``include/minfft_b200.h``.  This
+module loads them with ctypes and offers thin conveniences for Python
+callers (tests, the benchmark): every transform runs as CUDA kernels; there
+is no CPU implementation here, and loading fails loudly when the library has
+not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+from ._abi import FAMILIES, OP_FAMILY, OPS, MinfftLibrary, shapes
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+LIB_PATHS = {False: os.path.join(LIB_DIR, "libminfft_b200.so"), True: os.path.join(LIB_DIR, "libminfft_b200_single.so")}
+OP_CODES = {name: i for i, name in enumerate(OPS)}
+
+ERROR_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "EUNSUPPORTED", 5: "ETIMEOUT"}
+
+
+class MinfftError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"minfft_b200 error {ERROR_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class Engine(MinfftLibrary):
+    """One loaded engine library (one precision) with its extension API bound."""
+
+    def __init__(self, single: bool = False):
+        path = LIB_PATHS[bool(single)]
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing: build it with `python -m minfft_b200.build` "
+                              "(the engine has no CPU fallback)")
+        super().__init__(path, single)
+        L = self.lib
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
+        L.minfft_b200_last_error.restype = i32
+        L.minfft_b200_last_error.argtypes = []
+        L.minfft_b200_last_error_message.restype = ctypes.c_char_p
+        L.minfft_b200_last_error_message.argtypes = []
+        L.minfft_b200_set_stream.argtypes = [vp, vp]
+        L.minfft_b200_set_stream.restype = i32
+        L.minfft_b200_get_stream.argtypes = [vp]
+        L.minfft_b200_get_stream.restype = vp
+        L.minfft_b200_synchronize.argtypes = [vp]
+        L.minfft_b200_synchronize.restype = i32
+        L.minfft_b200_execute_batch.argtypes = [i32, vp, vp, i32, vp]
+        L.minfft_b200_execute_batch.restype = i32
+        for f in ("minfft_b200_input_bytes", "minfft_b200_output_bytes", "minfft_b200_launch_count"):
+            getattr(L, f).argtypes = [i32, vp]
+            getattr(L, f).restype = i64 if f != "minfft_b200_launch_count" else i32
+        L.minfft_b200_plan_bytes.argtypes = [vp]
+        L.minfft_b200_plan_bytes.restype = i64
+        L.minfft_b200_profile.argtypes = [vp, i32]
+        L.minfft_b200_profile.restype = i32
+        L.minfft_b200_profile_count.argtypes = [vp]
+        L.minfft_b200_profile_count.restype = i32
+        L.minfft_b200_profile_entry.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(i64),
+                                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.minfft_b200_profile_entry.restype = i32
+
+    # --------------------------------------------------------- errors
+    def last_error(self) -> int:
+        return int(self.lib.minfft_b200_last_error())
+
+    def last_error_message(self) -> str:
+        return self.lib.minfft_b200_last_error_message().decode()
+
+    def check(self) -> None:
+        """Raise MinfftError if the last call on this thread failed."""
+        code = self.last_error()
+        if code:
+            raise MinfftError(code, self.last_error_message())
+
+    # ------------------------------------------------------ extensions
+    def set_stream(self, aux: int, stream: int) -> None:
+        if self.lib.minfft_b200_set_stream(ctypes.c_void_p(aux), ctypes.c_void_p(stream or None)):
+            self.check()
+
+    def synchronize(self, aux: int) -> None:
+        if self.lib.minfft_b200_synchronize(ctypes.c_void_p(aux)):
+            self.check()
+
+    def execute_batch(self, op: str, x: int, y: int, howmany: int, aux: int) -> None:
+        rc = self.lib.minfft_b200_execute_batch(OP_CODES[op], ctypes.c_void_p(x), ctypes.c_void_p(y), howmany,
+                                                ctypes.c_void_p(aux))
+        if rc:
+            self.check()
+
+    def launch_count(self, op: str, aux: int) -> int:
+        return int(self.lib.minfft_b200_launch_count(OP_CODES[op], ctypes.c_void_p(aux)))
+
+    def plan_bytes(self, aux: int) -> int:
+        return int(self.lib.minfft_b200_plan_bytes(ctypes.c_void_p(aux)))
+
+    def profile(self, aux: int, enable: int) -> None:
+        if self.lib.minfft_b200_profile(ctypes.c_void_p(aux), int(enable)):
+            self.check()
+
+    def profile_stats(self, aux: int):
+        """[(label, launches, total_ms, bytes_per_launch)] recorded since profiling was enabled."""
+        n = self.lib.minfft_b200_profile_count(ctypes.c_void_p(aux))
+        if n < 0:
+            self.check()
+        out = []
+        for i in range(n):
+            lab, cnt, ms, by = ctypes.c_char_p(), ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+            if self.lib.minfft_b200_profile_entry(ctypes.c_void_p(aux), i, ctypes.byref(lab), ctypes.byref(cnt),
+                                                  ctypes.byref(ms), ctypes.byref(by)):
+                self.check()
+            out.append((lab.value.decode(), int(cnt.value), float(ms.value), float(by.value)))
+        return out
+
+    # ---------------------------------------------- checked plan API
+    def plan(self, family: str, dims: Sequence[int]) -> "Plan":
+        aux = self.mkaux(family, dims)
+        if not aux:
+            code = self.last_error()
+            raise MinfftError(code or 1, self.last_error_message() or f"maker returned NULL for {tuple(dims)}")
+        return Plan(self, family, tuple(int(d) for d in dims), aux)
+
+
+class Plan:
+    """An owned aux handle; ``plan(op, x, y)`` runs a transform on raw addresses."""
+
+    def __init__(self, engine: Engine, family: str, dims, aux: int):
+        self.engine, self.family, self.dims, self.aux = engine, family, dims, aux
+
+    def __call__(self, op: str, x: int, y: int, check: bool = True) -> None:
+        if OP_FAMILY[op] != self.family:
+            raise ValueError(f"{op} needs a {OP_FAMILY[op]} plan, this is a {self.family} plan")
+        self.engine.run(op, x, y, self.aux)
+        if check:
+            self.engine.check()
+
+    def batch(self, op: str, x: int, y: int, howmany: int) -> None:
+        self.engine.execute_batch(op, x, y, howmany, self.aux)
+
+    def set_stream(self, stream: int) -> None:
+        self.engine.set_stream(self.aux, stream)
+
+    def free(self) -> None:
+        if self.aux:
+            self.engine.free(self.aux)
+            self.aux = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+_engines = {}
+
+
+def engine(single: bool = False) -> Engine:
+    """The process-wide engine of the given precision (loaded on first use)."""
+    key = bool(single)
+    if key not in _engines:
+        _engines[key] = Engine(key)
+    return _engines[key]
+
+
+def torch_dtypes(single: bool):
+    import torch
+
+    return (torch.float32, torch.complex64) if single else (torch.float64, torch.complex128)
+
+
+def transform(op: str, x, dims: Optional[Sequence[int]] = None, single: Optional[bool] = None, out=None):
+    """Run ``op`` on a CUDA torch tensor through the C ABI and return the output tensor.
+
+    ``dims`` defaults to ``x.shape`` (to the real shape for invrealdft it must
+    be given).  The call is stream-ordered on the legacy default stream.
+    """
+    import torch
+
+    if single is None:
+        single = x.dtype in (torch.float32, torch.complex64)
+    if dims is None:
+        if op == "invrealdft":
+            raise ValueError("invrealdft needs the real dims")
+        dims = tuple(x.shape)
+    in_shape, in_c, out_shape, out_c = shapes(op, dims)
+    rdt, cdt = torch_dtypes(single)
+    x = x.to(dtype=cdt if in_c else rdt).contiguous().reshape(in_shape)
+    if out is None:
+        out = torch.empty(out_shape, dtype=cdt if out_c else rdt, device=x.device)
+    eng = engine(single)
+    p = eng.plan(OP_FAMILY[op], dims)
+    try:
+        p(op, x.data_ptr(), out.data_ptr())
+    finally:
+        p.free()
+    return out
+
+
+__all__ = ["ERROR_NAMES", "Engine", "Plan", "MinfftError", "engine", "transform", "shapes", "OPS", "FAMILIES", "OP_FAMILY",
+           "OP_CODES", "LIB_PATHS"]

@@ -1,0 +1,590 @@
+// One "axis pass": a batch of power-of-two complex DFTs of length L, each
+// computed by one group of L/R threads of a CTA, with the pre- and
+// post-processing of the transform kind fused into the load and the store.
+//
+// Addressing.  Transform b of the batch is split as b0 = b % d0,
+// b1 = (b / d0) % d1, b2 = b / (d0*d1); its input starts at
+// b0*is0 + b1*is1 + b2*is2 and element n sits at +n*in_n (likewise for the
+// output with os*, out_k).  This one form covers rows (in_n = 1), columns of
+// a C-order array (in_n = product of trailing dims) and the large-length
+// passes of a Stockham FFT over HBM (see plan.cu).
+//
+// Thread layout.  Row mode: the L/R threads of one transform are adjacent,
+// so a warp reads consecutive elements of one row.  Column mode: the cpb
+// transforms of the CTA are adjacent in memory (consecutive columns), so the
+// thread index runs fastest over the transform.  Either way every global
+// access of a warp is a contiguous run.
+//
+// Within the CTA the DFT is a Stockham autosort FFT: thread j of a transform
+// holds elements j + r*(L/R), r < R, in registers; each pass multiplies by
+// table twiddles, runs an R-point (or smaller) DFT in registers and exchanges
+// through padded shared memory.  The last pass leaves output element
+// k = j + r*(L/R) in register r, so the first load and the last store need
+// no shared memory at all for the plain complex transform.
+#pragma once
+
+#include "common.cuh"
+
+namespace mb {
+
+struct AxisParams {
+  const void* in;
+  void* out;
+  int64_t nbatch;
+  int64_t d0, d1;
+  int64_t is0, is1, is2;
+  int64_t os0, os1, os2;
+  int64_t in_n, out_k;
+  const cpx* tw;     // w_L^m, m < L (forward roots for the in-CTA passes)
+  const cpx* t1;     // kind table 1 (see the load/store stages)
+  const cpx* t2;     // kind table 2
+  const cpx* st_hi;  // large-length pass roots: w_Lt^(a << st_lobits)
+  const cpx* st_lo;  // large-length pass roots: w_Lt^c, c < 2^st_lobits
+  int64_t st_ns;     // span of the preceding HBM passes (1: no pre-twiddle)
+  int64_t st_div;    // elements per span index (product of trailing dims)
+  int st_shift;      // log2(Lt / (st_ns * L))
+  int st_lobits;
+  int cpb;      // transforms per CTA
+  int colmode;  // 1: thread index runs fastest over the transform
+  int flags;
+  int pad_;
+};
+
+enum : int {
+  F_CONJ_IN = 1,      // conjugate the input (inverse DFT = conj . DFT . conj)
+  F_CONJ_OUT = 2,     // conjugate the output
+  F_DST = 4,          // sine variant of a real symmetric transform
+  F_STAGE_ROWS = 8,   // store through shared memory with k running fastest
+  F_VEC = 16,         // real rows are aligned for paired (complex) vector access
+};
+
+// Shared-memory tile: cpb transforms of L complex values, padded every 16
+// elements so strided Stockham scatters spread over all banks.
+struct Tile {
+  cpx* s;
+  int cpb;
+  int colmode;
+  int lp;
+  __device__ __forceinline__ int idx(int c, int p) const { return colmode ? pad16(p) * cpb + c : c * lp + pad16(p); }
+};
+
+// Per-thread context: which transform, which thread within it, offsets.
+struct Ctx {
+  int64_t b;
+  int64_t b0;
+  int64_t oin, oout;
+  int c, j;
+  bool active;
+};
+
+__device__ __forceinline__ void batch_offsets(const AxisParams& p, int64_t b, int64_t& b0, int64_t& oi, int64_t& oo) {
+  b0 = b % p.d0;
+  const int64_t r = b / p.d0;
+  const int64_t b1 = r % p.d1;
+  const int64_t b2 = r / p.d1;
+  oi = b0 * p.is0 + b1 * p.is1 + b2 * p.is2;
+  oo = b0 * p.os0 + b1 * p.os1 + b2 * p.os2;
+}
+
+// ------------------------------------------------------------ Stockham core
+template <int L, int R, int RP, int NS>
+__device__ __forceinline__ void pass_compute(cpx (&v)[R], int j, const cpx* __restrict__ tw) {
+  constexpr int S = R / RP;  // sub-DFTs per thread in this pass
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    cpx u[RP];
+#pragma unroll
+    for (int r = 0; r < RP; ++r) u[r] = v[s + r * S];
+    if constexpr (NS > 1) {
+      const int jp = j + s * (L / R);
+      const int q = jp & (NS - 1);
+      constexpr int step = L / (NS * RP);
+#pragma unroll
+      for (int r = 1; r < RP; ++r) u[r] = cmul(u[r], ldg(tw + q * r * step));
+    }
+    fft_reg<RP>(u);
+#pragma unroll
+    for (int r = 0; r < RP; ++r) v[s + r * S] = u[r];
+  }
+}
+
+template <int L, int R, int RP, int NS>
+__device__ __forceinline__ void pass_scatter(const cpx (&v)[R], int j, int c, const Tile& t) {
+  constexpr int S = R / RP;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int jp = j + s * (L / R);
+    const int base = (jp / NS) * (NS * RP) + (jp & (NS - 1));
+#pragma unroll
+    for (int r = 0; r < RP; ++r) t.s[t.idx(c, base + r * NS)] = v[s + r * S];
+  }
+}
+
+template <int L, int R>
+__device__ __forceinline__ void gather_natural(cpx (&v)[R], int j, int c, const Tile& t) {
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = t.s[t.idx(c, j + r * (L / R))];
+}
+
+template <int L, int R>
+__device__ __forceinline__ void scatter_natural(const cpx (&v)[R], int j, int c, const Tile& t) {
+#pragma unroll
+  for (int r = 0; r < R; ++r) t.s[t.idx(c, j + r * (L / R))] = v[r];
+}
+
+template <int L, int R, int NS>
+__device__ __forceinline__ void run_passes(cpx (&v)[R], int j, int c, const Tile& t, const cpx* __restrict__ tw) {
+  constexpr int RP = (L / NS >= R) ? R : (L / NS);
+  pass_compute<L, R, RP, NS>(v, j, tw);
+  if constexpr (NS * RP < L) {
+    __syncthreads();
+    pass_scatter<L, R, RP, NS>(v, j, c, t);
+    __syncthreads();
+    gather_natural<L, R>(v, j, c, t);
+    run_passes<L, R, NS * RP>(v, j, c, t, tw);
+  }
+}
+
+// ---------------------------------------------------------------- load ops
+// Each load op fills v[r] with complex input element n = j + r*(L/R) of the
+// length-L DFT of transform x.b.
+
+// Plain complex input; optional conjugation and large-length pre-twiddle.
+struct LoadCplx {
+  static constexpr bool kStaged = false;
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+    const cpx* in = static_cast<const cpx*>(p.in) + x.oin;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t n = x.j + r * (L / R);
+      v[r] = x.active ? in[n * p.in_n] : czero();
+    }
+    if (p.flags & F_CONJ_IN) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r].y = -v[r].y;
+    }
+    if (p.st_ns > 1) {
+      // element n of span index q is multiplied by w_Lt^(q*n*Lt/(st_ns*L)),
+      // read as the product of a coarse and a fine table entry
+      const int64_t q = (x.b0 / p.st_div) & (p.st_ns - 1);
+      const int64_t lomask = (int64_t(1) << p.st_lobits) - 1;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int64_t n = x.j + r * (L / R);
+        const int64_t g = (q * n) << p.st_shift;
+        const cpx w = cmul(ldg(p.st_hi + (g >> p.st_lobits)), ldg(p.st_lo + (g & lomask)));
+        v[r] = cmul(v[r], w);
+      }
+    }
+  }
+};
+
+// Real row read as L complex pairs (x[2n], x[2n+1]): the half-length complex
+// DFT of the real DFT (reference minfft.c:541-543).
+struct LoadR2C {
+  static constexpr bool kStaged = false;
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+    const real* in = static_cast<const real*>(p.in) + x.oin;
+    const bool vec = (p.flags & F_VEC) != 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int n = x.j + r * (L / R);
+      if (!x.active)
+        v[r] = czero();
+      else if (vec)
+        v[r] = reinterpret_cast<const cpx*>(in)[n];
+      else
+        v[r] = cmk(in[2 * n], in[2 * n + 1]);
+    }
+  }
+};
+
+// Type-2 input permutation (reference minfft.c:707-710, 756-759): the
+// length-N sequence u_i = x[2i] (i < N/2), u_i = +-x[2N-1-2i] (i >= N/2)
+// read as complex pairs (u_2m, u_2m+1); N = 2L.
+struct LoadDCT2 {
+  static constexpr bool kStaged = false;
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+    const real* in = static_cast<const real*>(p.in) + x.oin;
+    const real sg = (p.flags & F_DST) ? real(-1) : real(1);
+    constexpr int N = 2 * L;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int m = x.j + r * (L / R);
+      if (!x.active) {
+        v[r] = czero();
+        continue;
+      }
+      const int i0 = 2 * m, i1 = 2 * m + 1;
+      const real a = i0 < L ? in[int64_t(2 * i0) * p.in_n] : sg * in[int64_t(2 * N - 1 - 2 * i0) * p.in_n];
+      const real b = i1 < L ? in[int64_t(2 * i1) * p.in_n] : sg * in[int64_t(2 * N - 1 - 2 * i1) * p.in_n];
+      v[r] = cmk(a, b);
+    }
+  }
+};
+
+// Type-4 pre-rotation (reference minfft.c:906-910, 953-957):
+// t_n = e_n (x[2n] + i x[N-1-2n]) for DCT-4, -e_n (x[2n] - i x[N-1-2n]) for
+// DST-4, with e_n = w_2N^n from table t1.
+struct LoadT4 {
+  static constexpr bool kStaged = false;
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+    const real* in = static_cast<const real*>(p.in) + x.oin;
+    const bool dst = (p.flags & F_DST) != 0;
+    constexpr int N = 2 * L;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int n = x.j + r * (L / R);
+      if (!x.active) {
+        v[r] = czero();
+        continue;
+      }
+      const real a = in[int64_t(2 * n) * p.in_n];
+      const real b = in[int64_t(N - 1 - 2 * n) * p.in_n];
+      const cpx e = ldg(p.t1 + n);
+      if (!dst) {
+        v[r] = cmul(e, cmk(a, b));
+      } else {
+        const cpx q = cmul(e, cmk(a, -b));
+        v[r] = cmk(-q.x, -q.y);
+      }
+    }
+  }
+};
+
+// Packing step of the inverse real DFT (reference minfft.c:628-656) for the
+// spectrum pair (z_k, z_{L-k}); returns t_k and t_{L-k}.  f = w_N^k.
+__device__ __forceinline__ void pack_pair(cpx za, cpx zb, cpx f, cpx& ta, cpx& tb) {
+  const cpx m = cconj(zb);
+  const cpx u = cadd(za, m);
+  const cpx d = csub(za, m);
+  const cpx vv = cmul(d, cmk(f.y, f.x));  // times i*conj(f)
+  ta = cadd(u, vv);
+  tb = cconj(csub(u, vv));
+}
+
+// Unpacking step of the real DFT (reference minfft.c:556-575) for the pair
+// (Z_k, Z_{L-k}) of the half-length DFT; returns X_k and X_{L-k}.
+__device__ __forceinline__ void unpack_pair(cpx za, cpx zb, cpx f, cpx& xa, cpx& xb) {
+  const cpx m = cconj(zb);
+  const real h = real(0.5);
+  const cpx u = cscale(cadd(za, m), h);
+  const cpx d = csub(za, m);
+  const cpx vv = cscale(cmul(d, cmk(f.y, -f.x)), h);  // times f/(2i)
+  xa = cadd(u, vv);
+  xb = cconj(csub(u, vv));
+}
+
+// Inverse real DFT input: spectrum X_k, k = 0..L, packed into L complex
+// values, staged in shared memory.  Stored conjugated: the inverse DFT is
+// computed as conj(DFT(conj(t))).  t2 = w_N^k, k < L/2.
+struct LoadC2R {
+  static constexpr bool kStaged = true;
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
+    const cpx* in = static_cast<const cpx*>(p.in) + x.oin;
+    for (int k = x.j; k <= L / 2; k += L / R) {
+      cpx z0 = czero(), z1 = czero();
+      if (x.active) {
+        z0 = in[int64_t(k) * p.in_n];
+        z1 = in[int64_t(L - k) * p.in_n];
+      }
+      if (k == 0) {
+        t.s[t.idx(x.c, 0)] = cmk(z0.x + z1.x, -(z0.x - z1.x));
+      } else if (2 * k == L) {
+        t.s[t.idx(x.c, k)] = cmk(2 * z0.x, 2 * z0.y);
+      } else {
+        cpx ta, tb;
+        pack_pair(z0, z1, ldg(p.t2 + k), ta, tb);
+        t.s[t.idx(x.c, k)] = cconj(ta);
+        t.s[t.idx(x.c, L - k)] = cconj(tb);
+      }
+    }
+    __syncthreads();
+    gather_natural<L, R>(v, x.j, x.c, t);
+  }
+};
+
+// Type-3 input (reference minfft.c:807-817, 857-867) followed by the
+// inverse-real-DFT packing, staged in shared memory (conjugated as above).
+// t1 = w_4N^n (n < N/2), t2 = w_N^k (k < L/2); N = 2L.
+struct LoadDCT3 {
+  static constexpr bool kStaged = true;
+  static __device__ __forceinline__ cpx zval(const real* in, int64_t s, int n, int L, bool dst, const cpx* e) {
+    const int N = 2 * L;
+    if (n == 0) return cmk(dst ? in[int64_t(N - 1) * s] : in[0], real(0));
+    if (n == L) {
+      const real r2 = real(1.414213562373095048801688724209698079);
+      return cmk(r2 * (dst ? in[int64_t(L - 1) * s] : in[int64_t(L) * s]), real(0));
+    }
+    const real a = dst ? in[int64_t(N - n - 1) * s] : in[int64_t(n) * s];
+    const real b = dst ? in[int64_t(n - 1) * s] : in[int64_t(N - n) * s];
+    return cconj(cmul(cmk(a, b), ldg(e + n)));
+  }
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
+    const real* in = static_cast<const real*>(p.in) + x.oin;
+    const bool dst = (p.flags & F_DST) != 0;
+    for (int k = x.j; k <= L / 2; k += L / R) {
+      cpx z0 = czero(), z1 = czero();
+      if (x.active) {
+        z0 = zval(in, p.in_n, k, L, dst, p.t1);
+        z1 = zval(in, p.in_n, L - k, L, dst, p.t1);
+      }
+      if (k == 0) {
+        t.s[t.idx(x.c, 0)] = cmk(z0.x + z1.x, -(z0.x - z1.x));
+      } else if (2 * k == L) {
+        t.s[t.idx(x.c, k)] = cmk(2 * z0.x, 2 * z0.y);
+      } else {
+        cpx ta, tb;
+        pack_pair(z0, z1, ldg(p.t2 + k), ta, tb);
+        t.s[t.idx(x.c, k)] = cconj(ta);
+        t.s[t.idx(x.c, L - k)] = cconj(tb);
+      }
+    }
+    __syncthreads();
+    gather_natural<L, R>(v, x.j, x.c, t);
+  }
+};
+
+// --------------------------------------------------------------- store ops
+// Each store op receives output element k = j + r*(L/R) of the length-L DFT
+// in v[r].
+
+// Offsets of the CTA's transforms, kept in shared memory so staged stores
+// can address any transform of the tile.
+struct TileOffsets {
+  int64_t* in_off;
+  int64_t* out_off;
+};
+
+struct StoreCplx {
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, const TileOffsets& to,
+                                             cpx (&v)[R]) {
+    cpx* out = static_cast<cpx*>(p.out);
+    const bool cj = (p.flags & F_CONJ_OUT) != 0;
+    if (!(p.flags & F_STAGE_ROWS)) {
+      if (!x.active) return;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int64_t k = x.j + r * (L / R);
+        cpx o = v[r];
+        if (cj) o.y = -o.y;
+        out[x.oout + k * p.out_k] = o;
+      }
+      return;
+    }
+    // staged: each transform's L outputs written with k running fastest
+    __syncthreads();
+    scatter_natural<L, R>(v, x.j, x.c, t);
+    __syncthreads();
+    const int total = p.cpb * L;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int c = e / L, k = e - c * L;
+      const int64_t b = int64_t(blockIdx.x) * p.cpb + c;
+      if (b >= p.nbatch) continue;
+      cpx o = t.s[t.idx(c, k)];
+      if (cj) o.y = -o.y;
+      out[to.out_off[c] + int64_t(k) * p.out_k] = o;
+    }
+  }
+};
+
+// Real DFT output (reference minfft.c:547-578): L+1 complex values from the
+// half-length DFT, via the pair unpacking; t1 = w_N^k, k < L/2.
+struct StoreR2C {
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, const TileOffsets&,
+                                             cpx (&v)[R]) {
+    __syncthreads();
+    scatter_natural<L, R>(v, x.j, x.c, t);
+    __syncthreads();
+    if (!x.active) return;
+    cpx* out = static_cast<cpx*>(p.out) + x.oout;
+    for (int k = x.j; k <= L / 2; k += L / R) {
+      const cpx za = t.s[t.idx(x.c, k)];
+      if (k == 0) {
+        out[0] = cmk(za.x + za.y, real(0));
+        out[int64_t(L) * p.out_k] = cmk(za.x - za.y, real(0));
+      } else if (2 * k == L) {
+        out[int64_t(k) * p.out_k] = cconj(za);
+      } else {
+        cpx xa, xb;
+        unpack_pair(za, t.s[t.idx(x.c, L - k)], ldg(p.t1 + k), xa, xb);
+        out[int64_t(k) * p.out_k] = xa;
+        out[int64_t(L - k) * p.out_k] = xb;
+      }
+    }
+  }
+};
+
+// Type-2 output (reference minfft.c:714-725, 763-774): real-DFT unpacking,
+// then y_n = 2 Re(V_n e_n), y_{N-n} = -2 Im(V_n e_n) (DCT-2; DST-2 maps the
+// same values to reversed positions).  t1 = w_4N^n (n < N/2), t2 = w_N^k.
+struct StoreDCT2 {
+  static __device__ __forceinline__ void emit(real* out, int64_t s, int n, int N, bool dst, cpx V, cpx e) {
+    const cpx q = cmul(V, e);
+    if (!dst) {
+      out[int64_t(n) * s] = 2 * q.x;
+      out[int64_t(N - n) * s] = -2 * q.y;
+    } else {
+      out[int64_t(n - 1) * s] = -2 * q.y;
+      out[int64_t(N - n - 1) * s] = 2 * q.x;
+    }
+  }
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, const TileOffsets&,
+                                             cpx (&v)[R]) {
+    __syncthreads();
+    scatter_natural<L, R>(v, x.j, x.c, t);
+    __syncthreads();
+    if (!x.active) return;
+    real* out = static_cast<real*>(p.out) + x.oout;
+    const bool dst = (p.flags & F_DST) != 0;
+    constexpr int N = 2 * L;
+    const real r2 = real(1.414213562373095048801688724209698079);
+    for (int k = x.j; k <= L / 2; k += L / R) {
+      const cpx za = t.s[t.idx(x.c, k)];
+      if (k == 0) {
+        const real v0 = za.x + za.y, vl = za.x - za.y;
+        out[int64_t(dst ? N - 1 : 0) * p.out_k] = 2 * v0;
+        out[int64_t(dst ? L - 1 : L) * p.out_k] = r2 * vl;
+      } else if (2 * k == L) {
+        emit(out, p.out_k, k, N, dst, cconj(za), ldg(p.t1 + k));
+      } else {
+        cpx xa, xb;
+        unpack_pair(za, t.s[t.idx(x.c, L - k)], ldg(p.t2 + k), xa, xb);
+        emit(out, p.out_k, k, N, dst, xa, ldg(p.t1 + k));
+        emit(out, p.out_k, L - k, N, dst, xb, ldg(p.t1 + L - k));
+      }
+    }
+  }
+};
+
+// Inverse real DFT output: the inverse half-length DFT (conjugate of the
+// forward result) read as interleaved reals (reference minfft.c:605,658).
+struct StoreC2R {
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, const TileOffsets&,
+                                             cpx (&v)[R]) {
+    if (!x.active) return;
+    real* out = static_cast<real*>(p.out) + x.oout;
+    const bool vec = (p.flags & F_VEC) != 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int m = x.j + r * (L / R);
+      const cpx w = cconj(v[r]);
+      if (vec) {
+        reinterpret_cast<cpx*>(out)[m] = w;
+      } else {
+        out[2 * m] = w.x;
+        out[2 * m + 1] = w.y;
+      }
+    }
+  }
+};
+
+// Type-3 output (reference minfft.c:821-824, 871-874): the inverse real
+// DFT's reals t_i go to y[2i] (i < N/2) and y[2N-1-2i] (i >= N/2, negated
+// for DST-3).
+struct StoreDCT3 {
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, const TileOffsets&,
+                                             cpx (&v)[R]) {
+    if (!x.active) return;
+    real* out = static_cast<real*>(p.out) + x.oout;
+    const bool dst = (p.flags & F_DST) != 0;
+    constexpr int N = 2 * L;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int m = x.j + r * (L / R);
+      const cpx w = cconj(v[r]);
+      const int i0 = 2 * m, i1 = 2 * m + 1;
+      const real a = (dst && i0 >= L) ? -w.x : w.x;
+      const real b = (dst && i1 >= L) ? -w.y : w.y;
+      out[int64_t(i0 < L ? 2 * i0 : 2 * N - 1 - 2 * i0) * p.out_k] = a;
+      out[int64_t(i1 < L ? 2 * i1 : 2 * N - 1 - 2 * i1) * p.out_k] = b;
+    }
+  }
+};
+
+// Type-4 post-rotation (reference minfft.c:916-921, 963-968): T_m feeds
+// y[2m] = 2 Re(g_2m T_m) and y[N-1-2m] = 2 Re(g_{N-1-2m} conj(T_m)) (Im for
+// DST-4), g_q = w_8N^(2q+1) from table t2.
+struct StoreT4 {
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, const TileOffsets&,
+                                             cpx (&v)[R]) {
+    if (!x.active) return;
+    real* out = static_cast<real*>(p.out) + x.oout;
+    const bool dst = (p.flags & F_DST) != 0;
+    constexpr int N = 2 * L;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int m = x.j + r * (L / R);
+      const cpx T = v[r];
+      const cpx a = cmul(ldg(p.t2 + 2 * m), T);
+      const cpx b = cmul(ldg(p.t2 + (N - 1 - 2 * m)), cconj(T));
+      out[int64_t(2 * m) * p.out_k] = 2 * (dst ? a.y : a.x);
+      out[int64_t(N - 1 - 2 * m) * p.out_k] = 2 * (dst ? b.y : b.x);
+    }
+  }
+};
+
+// ------------------------------------------------------------------ kernel
+template <int L>
+struct RadixFor {
+  static constexpr int value = L >= 16 ? 16 : L;
+};
+
+template <int L, class LoadOp, class StoreOp>
+__global__ void __launch_bounds__(512) axis_pass_kernel(const AxisParams p) {
+  constexpr int R = RadixFor<L>::value;
+  constexpr int TPT = L / R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int64_t* offs = reinterpret_cast<int64_t*>(smem_raw);
+  TileOffsets to{offs, offs + p.cpb};
+  Tile t{reinterpret_cast<cpx*>(smem_raw + 16 * ((2 * p.cpb * sizeof(int64_t) + 15) / 16)), p.cpb, p.colmode,
+         padded_len(L)};
+
+  // offsets of the CTA's transforms, computed once per transform
+  for (int c = threadIdx.x; c < p.cpb; c += blockDim.x) {
+    const int64_t b = int64_t(blockIdx.x) * p.cpb + c;
+    int64_t b0, oi, oo;
+    batch_offsets(p, b < p.nbatch ? b : 0, b0, oi, oo);
+    to.in_off[c] = oi;
+    to.out_off[c] = oo;
+  }
+  __syncthreads();
+
+  Ctx x;
+  if (p.colmode) {
+    x.c = threadIdx.x % p.cpb;
+    x.j = threadIdx.x / p.cpb;
+  } else {
+    x.j = threadIdx.x % TPT;
+    x.c = threadIdx.x / TPT;
+  }
+  x.b = int64_t(blockIdx.x) * p.cpb + x.c;
+  x.active = x.b < p.nbatch;
+  x.oin = to.in_off[x.c];
+  x.oout = to.out_off[x.c];
+  x.b0 = x.b % p.d0;
+
+  cpx v[R];
+  LoadOp::template run<L, R>(p, x, t, v);
+  run_passes<L, R, 1>(v, x.j, x.c, t, p.tw);
+  StoreOp::template run<L, R>(p, x, t, to, v);
+}
+
+// Number of bytes of dynamic shared memory the kernel needs for cpb transforms.
+inline size_t axis_pass_smem(int L, int cpb) {
+  return 16 * ((2 * cpb * sizeof(int64_t) + 15) / 16) + size_t(cpb) * padded_len(L) * sizeof(cpx);
+}
+
+}  // namespace mb

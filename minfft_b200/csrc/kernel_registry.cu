@@ -1,0 +1,27 @@
+// Dispatch from (combo, log2 L) to the instantiated axis-pass kernels; the
+// instantiations live in one translation unit per combo (kernels_*.cu) so
+// they compile in parallel.
+#include "kernel_registry.h"
+
+namespace mb {
+
+const void* axis_kernel_cplx(int log2L);
+const void* axis_kernel_r2c(int log2L);
+const void* axis_kernel_c2r(int log2L);
+const void* axis_kernel_dct2(int log2L);
+const void* axis_kernel_dct3(int log2L);
+const void* axis_kernel_t4(int log2L);
+
+const void* axis_kernel(int combo, int log2L) {
+  switch (combo) {
+    case K_CPLX: return axis_kernel_cplx(log2L);
+    case K_R2C: return axis_kernel_r2c(log2L);
+    case K_C2R: return axis_kernel_c2r(log2L);
+    case K_DCT2: return axis_kernel_dct2(log2L);
+    case K_DCT3: return axis_kernel_dct3(log2L);
+    case K_T4: return axis_kernel_t4(log2L);
+    default: return nullptr;
+  }
+}
+
+}  // namespace mb

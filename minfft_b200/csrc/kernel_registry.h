@@ -1,0 +1,22 @@
+// Kernel registry: every instantiated axis-pass kernel, addressed by the
+// (load stage, store stage) combination and log2 of its in-CTA DFT length.
+#pragma once
+
+namespace mb {
+
+enum Combo : int {
+  K_CPLX = 0,   // complex -> complex (DFT, inverse DFT via conjugation, HBM passes)
+  K_R2C,        // real DFT with fused unpacking
+  K_C2R,        // inverse real DFT with fused packing
+  K_DCT2,       // DCT-2 / DST-2 with fused permutation, unpacking and post-rotation
+  K_DCT3,       // DCT-3 / DST-3 with fused pre-rotation, packing and de-interleave
+  K_T4,         // DCT-4 / DST-4 with fused pre- and post-rotation
+  K_COUNT
+};
+
+constexpr int kMaxLog2L = 13;  // largest in-CTA DFT: 8192 points
+
+// Returns the kernel function for combo and log2(L), or nullptr.
+const void* axis_kernel(int combo, int log2L);
+
+}  // namespace mb

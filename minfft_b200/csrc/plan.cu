@@ -1,0 +1,1166 @@
+// Host side of the engine: plans ("aux") with device-resident root tables
+// and scratch, launch-list planning for every transform kind and
+// dimensionality, execution on a CUDA stream, and the C ABI of minfft.h and
+// minfft_b200.h.
+//
+// Planning model.  A transform is a sequence of "axis steps".  Each axis
+// step is one batched 1-D transform along one axis of a C-order array,
+// executed by
+//   * one axis-pass kernel when its half- or full-length complex DFT fits in
+//     one CTA (L <= 8192 points along contiguous rows, L <= 4096 along
+//     strided columns), with the kind's pre/post-processing fused in; or
+//   * a Stockham FFT over HBM: P passes of in-CTA sub-DFTs of length <= 4096,
+//     pass p reading with stride L/R_p and pre-multiplying by
+//     w_{Ns*R_p}^((j mod Ns)*r) (Ns = product of earlier radices), plus a
+//     standalone pre/post kernel for real kinds.
+// Multi-dimensional transforms apply the 1-D transform along every axis, as
+// the reference's transposing recursion does (minfft.c:33-72, 582-597,
+// 662-687); here each axis is processed in place in natural C order instead
+// of being transposed, which gives the same result.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "axis_pass.cuh"
+#include "kernel_registry.h"
+#include "line_kernels.h"
+#include "minfft.h"
+#include "minfft_b200.h"
+
+#define MB_EXPORT extern "C" __attribute__((visibility("default")))
+
+using mb::AxisParams;
+using mb::cpx;
+using mb::LineParams;
+using mb::real;
+
+// =============================================================== errors
+namespace {
+
+thread_local int g_err = 0;
+thread_local char g_msg[512] = "";
+
+void set_error(int code, const char* fmt, ...) {
+  g_err = code;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+  va_end(ap);
+}
+
+bool cuda_ok(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  set_error(e == cudaErrorMemoryAllocation ? MINFFT_B200_ENOMEM : MINFFT_B200_ECUDA, "%s: %s", what,
+            cudaGetErrorString(e));
+  return false;
+}
+
+// ========================================================== unit roots
+// (cos, sin)(2*pi*n/N), with the angle folded into [0, pi/4] before calling
+// libm -- the folding of reference minfft.c:989-1018, evaluated in double
+// for both precisions so the single-precision tables are correctly rounded.
+void unit_root(int64_t n, int64_t N, double* c, double* s) {
+  if (n < 0) {
+    unit_root(-n, N, c, s);
+    *s = -*s;
+  } else if (n >= N / 2) {
+    unit_root(n - N / 2, N, c, s);
+    *c = -*c;
+    *s = -*s;
+  } else if (n >= N / 4) {
+    double cc, ss;
+    unit_root(n - N / 4, N, &cc, &ss);
+    *c = -ss;
+    *s = cc;
+  } else if (n > N / 8) {
+    double cc, ss;
+    unit_root(N / 4 - n, N, &cc, &ss);
+    *c = ss;
+    *s = cc;
+  } else {
+    const double pi = 3.141592653589793238462643383279502884;
+    const double ang = 2 * pi * (double)n / (double)N;
+    *c = std::cos(ang);
+    *s = std::sin(ang);
+  }
+}
+
+// w_N^m = exp(-2*pi*i*m/N)
+cpx root_w(int64_t m, int64_t N) {
+  double c, s;
+  unit_root(-m, N, &c, &s);
+  cpx r;
+  r.x = (real)c;
+  r.y = (real)s;
+  return r;
+}
+
+int ilog2(int64_t v) {
+  int r = 0;
+  while ((int64_t(1) << r) < v) ++r;
+  return r;
+}
+
+bool is_pow2(int64_t v) { return v > 0 && (v & (v - 1)) == 0; }
+
+// =================================================== device properties
+struct DeviceInfo {
+  int max_smem = 48 * 1024;
+  int sms = 148;
+};
+
+DeviceInfo device_info(int dev) {
+  static std::mutex mu;
+  static std::map<int, DeviceInfo> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  DeviceInfo d;
+  int v = 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && v > 0) d.max_smem = v;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0) d.sms = v;
+  cache[dev] = d;
+  return d;
+}
+
+bool ensure_smem_attr(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<const void*, size_t> done;
+  if (bytes <= 48 * 1024) return true;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find(fn);
+  if (it != done.end() && it->second >= bytes) return true;
+  if (!cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+               "cudaFuncSetAttribute"))
+    return false;
+  done[fn] = bytes;
+  return true;
+}
+
+// ============================================================ programs
+enum Buf : int { BUF_X = 0, BUF_Y, BUF_T1, BUF_T2, BUF_T3, BUF_T4, BUF_COUNT };
+
+struct Launch {
+  const void* fn = nullptr;
+  unsigned grid = 0, block = 0;
+  size_t smem = 0;
+  int in_buf = BUF_X, out_buf = BUF_Y;
+  bool is_line = false;
+  bool vec_in = false;   // set F_VEC when the resolved real input is complex-aligned
+  bool vec_out = false;  // same for the real output
+  bool in_c = false;     // the kernel reads its input as complex values
+  bool out_c = false;    // the kernel writes its output as complex values
+  AxisParams ap;
+  LineParams lp;
+  std::string label;  // kernel and shape, for launch-level timing
+  double bytes = 0;   // algorithmic bytes: each input element read once, each output written once
+};
+
+struct Program {
+  std::vector<Launch> launches;
+  size_t tbytes[BUF_COUNT] = {0, 0, 0, 0, 0, 0};
+};
+
+enum Family : int { FAM_DFT = 0, FAM_REALDFT, FAM_T2T3, FAM_T4 };
+
+int op_family(int op) {
+  switch (op) {
+    case MINFFT_B200_DFT:
+    case MINFFT_B200_INVDFT: return FAM_DFT;
+    case MINFFT_B200_REALDFT:
+    case MINFFT_B200_INVREALDFT: return FAM_REALDFT;
+    case MINFFT_B200_DCT2:
+    case MINFFT_B200_DST2:
+    case MINFFT_B200_DCT3:
+    case MINFFT_B200_DST3: return FAM_T2T3;
+    case MINFFT_B200_DCT4:
+    case MINFFT_B200_DST4: return FAM_T4;
+    default: return -1;
+  }
+}
+
+// table kinds kept on the device by each plan
+enum TableKind : int { TB_TW = 0, TB_RFT, TB_T23, TB_T4PRE, TB_T4POST, TB_STHI, TB_STLO };
+
+}  // namespace
+
+// ================================================================ plan
+struct minfft_aux {
+  int family = 0;
+  std::vector<int> dims;
+  int64_t total = 1;  // product of dims
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::map<std::pair<int, int64_t>, void*> tables;
+  void* bufs[BUF_COUNT] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  size_t buf_bytes[BUF_COUNT] = {0, 0, 0, 0, 0, 0};
+  std::map<std::tuple<int, int, int>, Program> programs;  // (op, howmany, alias)
+  void* stage_in = nullptr;
+  size_t stage_in_bytes = 0;
+  void* stage_out = nullptr;
+  size_t stage_out_bytes = 0;
+  size_t table_bytes = 0;
+  // launch-level timing (minfft_b200_profile)
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  struct Pending {
+    const Launch* ln;
+    size_t e0, e1;
+  };
+  std::vector<Pending> pending;
+  struct Stat {
+    std::string label;
+    long long launches = 0;
+    double ms = 0;
+    double bytes = 0;
+  };
+  std::vector<Stat> stats;
+};
+
+namespace {
+
+int64_t st_lobits_for(int64_t Lt) { return (ilog2(Lt) + 1) / 2; }
+
+// Device table of the given kind for length N (built on first use).
+const cpx* table(minfft_aux* a, int kind, int64_t N) {
+  auto key = std::make_pair(kind, N);
+  auto it = a->tables.find(key);
+  if (it != a->tables.end()) return static_cast<const cpx*>(it->second);
+  std::vector<cpx> h;
+  switch (kind) {
+    case TB_TW:  // w_N^m, m < N
+      h.resize(N);
+      for (int64_t m = 0; m < N; ++m) h[m] = root_w(m, N);
+      break;
+    case TB_RFT:  // w_N^k, k < N/4 (real-DFT unpacking, minfft.c:1141-1144)
+      h.resize(std::max<int64_t>(N / 4, 1));
+      for (int64_t k = 0; k < (int64_t)h.size(); ++k) h[k] = root_w(k, N);
+      break;
+    case TB_T23:  // w_4N^n, n < N/2 (minfft.c:1229-1232)
+      h.resize(std::max<int64_t>(N / 2, 1));
+      for (int64_t n = 0; n < (int64_t)h.size(); ++n) h[n] = root_w(n, 4 * N);
+      break;
+    case TB_T4PRE:  // w_2N^n, n < N/2 (minfft.c:1291-1294)
+      h.resize(std::max<int64_t>(N / 2, 1));
+      for (int64_t n = 0; n < (int64_t)h.size(); ++n) h[n] = root_w(n, 2 * N);
+      break;
+    case TB_T4POST:  // w_8N^(2q+1), q < N (minfft.c:1295-1298)
+      h.resize(N);
+      for (int64_t q = 0; q < N; ++q) h[q] = root_w(2 * q + 1, 8 * N);
+      break;
+    case TB_STHI: {  // w_N^(a << lobits)
+      const int lb = (int)st_lobits_for(N);
+      h.resize(std::max<int64_t>(N >> lb, 1));
+      for (int64_t q = 0; q < (int64_t)h.size(); ++q) h[q] = root_w(q << lb, N);
+      break;
+    }
+    case TB_STLO: {  // w_N^c, c < 2^lobits
+      const int lb = (int)st_lobits_for(N);
+      h.resize(int64_t(1) << lb);
+      for (int64_t q = 0; q < (int64_t)h.size(); ++q) h[q] = root_w(q, N);
+      break;
+    }
+    default: return nullptr;
+  }
+  void* d = nullptr;
+  const size_t bytes = h.size() * sizeof(cpx);
+  if (!cuda_ok(cudaMalloc(&d, bytes), "cudaMalloc(table)")) return nullptr;
+  if (!cuda_ok(cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice), "cudaMemcpy(table)")) {
+    cudaFree(d);
+    return nullptr;
+  }
+  a->tables[key] = d;
+  a->table_bytes += bytes;
+  return static_cast<const cpx*>(d);
+}
+
+// ------------------------------------------------------------ planner
+constexpr int kRowCapLog2 = 13;  // in-CTA DFT along contiguous rows: <= 8192
+constexpr int kColCapLog2 = 12;  // along strided columns: <= 4096
+constexpr int kPassCapLog2 = 12; // sub-DFTs of the HBM passes: <= 4096
+
+struct AxisStep {
+  int combo;        // mb::Combo
+  int64_t N;        // axis length (real length for real kinds)
+  int64_t outer, inner;
+  int64_t in_row, out_row;  // elements between consecutive outer rows
+  int flags;
+  int in_buf, out_buf;
+};
+
+struct Planner {
+  minfft_aux* a;
+  Program* prog;
+  int dev_max_smem;
+  int sms;
+  bool ok = true;
+
+  void need(int buf, size_t bytes) { prog->tbytes[buf] = std::max(prog->tbytes[buf], bytes); }
+
+  const cpx* tab(int kind, int64_t N) {
+    const cpx* t = table(a, kind, N);
+    if (!t) ok = false;
+    return t;
+  }
+
+  // transforms per CTA for an in-CTA DFT of length L
+  int choose_cpb(int L, bool colmode) {
+    const int R = std::min(16, L);
+    const int tpt = L / R;
+    int cpb = std::max(1, 256 / tpt);
+    if (colmode) {
+      const int want = int(128 / sizeof(cpx));  // 128-byte runs of adjacent columns
+      if (cpb < want) cpb = std::max(cpb, std::min(want, std::max(1, 512 / tpt)));
+    }
+    while (cpb > 1 && mb::axis_pass_smem(L, cpb) > (size_t)dev_max_smem) cpb /= 2;
+    return cpb;
+  }
+
+  static bool staged(int combo) {
+    return combo == mb::K_R2C || combo == mb::K_C2R || combo == mb::K_DCT2 || combo == mb::K_DCT3;
+  }
+
+  void add_axis_kernel(int combo, int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, bool vec_in,
+                       bool vec_out) {
+    const int lg = ilog2(L);
+    Launch ln;
+    ln.fn = mb::axis_kernel(combo, lg);
+    if (!ln.fn) {
+      set_error(MINFFT_B200_EUNSUPPORTED, "no kernel for combo %d, L=%d", combo, L);
+      ok = false;
+      return;
+    }
+    const int R = std::min(16, L);
+    const int tpt = L / R;
+    const bool tile = (L > R) || staged(combo) || (ap.flags & mb::F_STAGE_ROWS);
+    ln.smem = tile ? mb::axis_pass_smem(L, ap.cpb) : size_t(16 * ((2 * ap.cpb * sizeof(int64_t) + 15) / 16));
+    if (ln.smem > (size_t)dev_max_smem) {
+      set_error(MINFFT_B200_EUNSUPPORTED, "shared memory %zu exceeds %d", ln.smem, dev_max_smem);
+      ok = false;
+      return;
+    }
+    if (!ensure_smem_attr(ln.fn, ln.smem)) {
+      ok = false;
+      return;
+    }
+    ap.nbatch = nbatch;
+    ln.block = unsigned(ap.cpb * tpt);
+    ln.grid = unsigned((nbatch + ap.cpb - 1) / ap.cpb);
+    ln.in_buf = in_buf;
+    ln.out_buf = out_buf;
+    ln.vec_in = vec_in;
+    ln.vec_out = vec_out;
+    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R);
+    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C);
+    ln.ap = ap;
+    {
+      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4"};
+      const double R = sizeof(real), C = sizeof(cpx);
+      double per = 0;
+      switch (combo) {
+        case mb::K_CPLX: per = 2.0 * L * C; break;
+        case mb::K_R2C: per = 2.0 * L * R + (L + 1) * C; break;
+        case mb::K_C2R: per = (L + 1) * C + 2.0 * L * R; break;
+        default: per = 4.0 * L * R; break;
+      }
+      ln.bytes = per * double(nbatch);
+      char buf[160];
+      snprintf(buf, sizeof(buf), "axis_pass<%s,L=%d,%s%s> batch=%lld", names[combo], L, ap.colmode ? "col" : "row",
+               ap.st_ns > 1 ? ",hbm" : "", (long long)nbatch);
+      ln.label = buf;
+    }
+    prog->launches.push_back(ln);
+  }
+
+  void add_line_kernel(int which, LineParams lp, int64_t items, int in_buf, int out_buf) {
+    Launch ln;
+    ln.fn = mb::line_kernel(which);
+    ln.is_line = true;
+    ln.block = 256;
+    const int64_t want = (items + 255) / 256;
+    ln.grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * 32)));
+    ln.in_buf = in_buf;
+    ln.out_buf = out_buf;
+    switch (which) {
+      case mb::LK_C2R_PACK:
+      case mb::LK_R2C_UNPACK: ln.in_c = ln.out_c = true; break;
+      case mb::LK_DCT2_PRE:
+      case mb::LK_T4_PRE:
+      case mb::LK_DCT3_PACK: ln.out_c = true; break;
+      case mb::LK_DCT2_POST:
+      case mb::LK_DCT3_POST:
+      case mb::LK_T4_POST: ln.in_c = true; break;
+      default:
+        ln.in_c = (lp.mode == mb::UNIT_CPLX_TO_REAL || lp.mode == mb::UNIT_COPY_CPLX);
+        ln.out_c = (lp.mode == mb::UNIT_REAL_TO_CPLX || lp.mode == mb::UNIT_COPY_CPLX);
+        break;
+    }
+    ln.lp = lp;
+    {
+      static const char* names[] = {"dct2_pre", "t4_pre", "c2r_pack", "dct3_pack", "r2c_unpack",
+                                    "dct2_post", "dct3_post", "t4_post", "unit"};
+      const double R = sizeof(real), C = sizeof(cpx);
+      const double lines = double(lp.outer) * double(lp.inner), L = double(lp.L);
+      switch (which) {
+        case mb::LK_DCT2_PRE:
+        case mb::LK_T4_PRE: ln.bytes = lines * (2 * L * R + L * C); break;
+        case mb::LK_DCT3_PACK: ln.bytes = lines * (2 * L * R + L * C); break;
+        case mb::LK_C2R_PACK: ln.bytes = lines * ((L + 1) * C + L * C); break;
+        case mb::LK_R2C_UNPACK: ln.bytes = lines * (L * C + (L + 1) * C); break;
+        case mb::LK_DCT2_POST:
+        case mb::LK_DCT3_POST:
+        case mb::LK_T4_POST: ln.bytes = lines * (L * C + 2 * L * R); break;
+        default: {
+          const double in_e = ln.in_c ? C : R, out_e = ln.out_c ? C : R;
+          ln.bytes = L * (in_e + out_e);
+        }
+      }
+      char buf[160];
+      snprintf(buf, sizeof(buf), "line<%s> items=%lld", names[which], (long long)items);
+      ln.label = buf;
+    }
+    prog->launches.push_back(ln);
+  }
+
+  void add_unit(int mode, int64_t count, real scale, int in_buf, int out_buf) {
+    LineParams lp{};
+    lp.L = count;
+    lp.mode = mode;
+    lp.scale = scale;
+    add_line_kernel(mb::LK_UNIT, lp, count, in_buf, out_buf);
+  }
+
+  AxisParams base_params() {
+    AxisParams ap;
+    memset(&ap, 0, sizeof(ap));
+    ap.d0 = ap.d1 = 1;
+    ap.st_ns = 1;
+    ap.st_div = 1;
+    return ap;
+  }
+
+  void set_kind_tables(AxisParams& ap, int combo, int64_t N) {
+    switch (combo) {
+      case mb::K_R2C: ap.t1 = tab(TB_RFT, N); break;
+      case mb::K_C2R: ap.t2 = tab(TB_RFT, N); break;
+      case mb::K_DCT2:
+      case mb::K_DCT3:
+        ap.t1 = tab(TB_T23, N);
+        ap.t2 = tab(TB_RFT, N);
+        break;
+      case mb::K_T4:
+        ap.t1 = tab(TB_T4PRE, N);
+        ap.t2 = tab(TB_T4POST, N);
+        break;
+      default: break;
+    }
+  }
+
+  int pick_temp(std::initializer_list<int> exclude) {
+    for (int b : {BUF_T2, BUF_T3, BUF_T4}) {
+      bool bad = false;
+      for (int e : exclude) bad |= (e == b);
+      if (!bad) return b;
+    }
+    return BUF_T4;
+  }
+
+  void plan_axis(const AxisStep& s) {
+    const size_t R_ = sizeof(real), C_ = sizeof(cpx);
+    if (s.N == 1) {
+      const int64_t cnt = s.outer * s.inner;
+      const real r2 = real(1.414213562373095048801688724209698079);
+      switch (s.combo) {
+        case mb::K_CPLX:
+          if (s.in_buf != s.out_buf) add_unit(mb::UNIT_COPY_CPLX, cnt, 1, s.in_buf, s.out_buf);
+          break;
+        case mb::K_R2C: add_unit(mb::UNIT_REAL_TO_CPLX, cnt, 1, s.in_buf, s.out_buf); break;
+        case mb::K_C2R: add_unit(mb::UNIT_CPLX_TO_REAL, cnt, 1, s.in_buf, s.out_buf); break;
+        case mb::K_DCT2: add_unit(mb::UNIT_SCALE_REAL, cnt, 2, s.in_buf, s.out_buf); break;
+        case mb::K_DCT3:
+          if (s.in_buf != s.out_buf) add_unit(mb::UNIT_SCALE_REAL, cnt, 1, s.in_buf, s.out_buf);
+          break;
+        case mb::K_T4: add_unit(mb::UNIT_SCALE_REAL, cnt, r2, s.in_buf, s.out_buf); break;
+      }
+      (void)R_;
+      (void)C_;
+      return;
+    }
+    const int64_t L = (s.combo == mb::K_CPLX) ? s.N : s.N / 2;
+    const bool colmode = s.inner > 1;
+    const int cap = colmode ? kColCapLog2 : kRowCapLog2;
+    if (ilog2(L) <= cap) {
+      AxisParams ap = base_params();
+      ap.d0 = s.inner;
+      ap.d1 = s.outer;
+      ap.is0 = 1;
+      ap.is1 = s.in_row;
+      ap.in_n = s.inner;
+      ap.os0 = 1;
+      ap.os1 = s.out_row;
+      ap.out_k = s.inner;
+      ap.colmode = colmode ? 1 : 0;
+      ap.cpb = choose_cpb((int)L, colmode);
+      ap.flags = s.flags;
+      ap.tw = tab(TB_TW, L);
+      set_kind_tables(ap, s.combo, s.N);
+      add_axis_kernel(s.combo, (int)L, s.outer * s.inner, ap, s.in_buf, s.out_buf, s.combo == mb::K_R2C,
+                      s.combo == mb::K_C2R);
+      return;
+    }
+    plan_multipass(s, L);
+  }
+
+  // Stockham FFT over HBM for a long axis (see the file comment).
+  void plan_multipass(const AxisStep& s, int64_t Lt) {
+    const int bits = ilog2(Lt);
+    const int P = (bits + kPassCapLog2 - 1) / kPassCapLog2;
+    std::vector<int> pb(P, bits / P);
+    for (int p = 0; p < bits % P; ++p) pb[p] += 1;
+    const int64_t inner = s.inner, outer = s.outer;
+    const int64_t Lp = Lt * inner;
+    const size_t work_bytes = size_t(outer) * size_t(Lp) * sizeof(cpx);
+    const bool inverse_cplx = (s.combo == mb::K_CPLX) && (s.flags & mb::F_CONJ_IN);
+    const bool conj_chain = inverse_cplx || s.combo == mb::K_C2R || s.combo == mb::K_DCT3;
+
+    // --- pre-processing: chain source
+    int cs = s.in_buf;
+    auto line = [&](int64_t in_so, int64_t in_sn, int64_t out_so, int64_t out_sn) {
+      LineParams lp{};
+      lp.outer = outer;
+      lp.inner = inner;
+      lp.L = Lt;
+      lp.in_so = in_so;
+      lp.in_sn = in_sn;
+      lp.out_so = out_so;
+      lp.out_sn = out_sn;
+      lp.flags = s.flags;
+      return lp;
+    };
+    if (s.combo == mb::K_DCT2 || s.combo == mb::K_T4 || s.combo == mb::K_C2R || s.combo == mb::K_DCT3) {
+      cs = BUF_T2;
+      need(cs, work_bytes);
+      LineParams lp = line(s.in_row, inner, Lp, inner);
+      int which = 0;
+      int64_t items = outer * inner * Lt;
+      if (s.combo == mb::K_DCT2) {
+        which = mb::LK_DCT2_PRE;
+      } else if (s.combo == mb::K_T4) {
+        which = mb::LK_T4_PRE;
+        lp.t1 = tab(TB_T4PRE, s.N);
+      } else if (s.combo == mb::K_C2R) {
+        which = mb::LK_C2R_PACK;
+        lp.t2 = tab(TB_RFT, s.N);
+        items = outer * inner * (Lt / 2 + 1);
+      } else {
+        which = mb::LK_DCT3_PACK;
+        lp.t1 = tab(TB_T23, s.N);
+        lp.t2 = tab(TB_RFT, s.N);
+        items = outer * inner * (Lt / 2 + 1);
+      }
+      add_line_kernel(which, lp, items, s.in_buf, cs);
+    }
+    const bool post = (s.combo == mb::K_R2C || s.combo == mb::K_DCT2 || s.combo == mb::K_DCT3 || s.combo == mb::K_T4);
+
+    // --- the HBM passes
+    int prev = cs;
+    int64_t Ns = 1;
+    int last_src = cs;
+    int cd = s.out_buf;
+    for (int p = 0; p < P; ++p) {
+      const int64_t Rp = int64_t(1) << pb[p];
+      const bool last = (p == P - 1);
+      int dst;
+      if (!last) {
+        dst = pick_temp({prev});
+        need(dst, work_bytes);
+      } else if (post) {
+        dst = pick_temp({prev});
+        need(dst, work_bytes);
+        cd = dst;
+      } else {
+        dst = s.out_buf;
+      }
+      const int64_t Nsp = Ns * inner;
+      AxisParams ap = base_params();
+      ap.d0 = Nsp;
+      ap.d1 = Lt / (Ns * Rp);
+      ap.is0 = 1;
+      ap.is1 = Nsp;
+      ap.is2 = Lp;
+      ap.in_n = Lp / Rp;
+      ap.os0 = 1;
+      ap.os1 = Nsp * Rp;
+      ap.os2 = Lp;
+      ap.out_k = Nsp;
+      ap.st_ns = Ns;
+      ap.st_div = inner;
+      ap.st_shift = ilog2(Lt / (Ns * Rp));
+      ap.st_lobits = (int)st_lobits_for(Lt);
+      if (Ns > 1) {
+        ap.st_hi = tab(TB_STHI, Lt);
+        ap.st_lo = tab(TB_STLO, Lt);
+      }
+      ap.colmode = 1;
+      ap.cpb = choose_cpb((int)Rp, true);
+      ap.flags = 0;
+      if (Nsp == 1) ap.flags |= mb::F_STAGE_ROWS;
+      if (p == 0 && inverse_cplx) ap.flags |= mb::F_CONJ_IN;
+      if (last && conj_chain && s.combo != mb::K_DCT3) ap.flags |= mb::F_CONJ_OUT;
+      ap.tw = tab(TB_TW, Rp);
+      add_axis_kernel(mb::K_CPLX, (int)Rp, outer * (Lp / Rp), ap, prev, dst, false, false);
+      last_src = prev;
+      prev = dst;
+      Ns *= Rp;
+    }
+    (void)last_src;
+
+    // --- post-processing
+    if (post) {
+      LineParams lp = line(Lp, inner, s.out_row, inner);
+      int which = 0;
+      int64_t items = outer * inner * (Lt / 2 + 1);
+      if (s.combo == mb::K_R2C) {
+        which = mb::LK_R2C_UNPACK;
+        lp.t1 = tab(TB_RFT, s.N);
+      } else if (s.combo == mb::K_DCT2) {
+        which = mb::LK_DCT2_POST;
+        lp.t1 = tab(TB_T23, s.N);
+        lp.t2 = tab(TB_RFT, s.N);
+      } else if (s.combo == mb::K_DCT3) {
+        which = mb::LK_DCT3_POST;
+        items = outer * inner * Lt;
+      } else {
+        which = mb::LK_T4_POST;
+        lp.t2 = tab(TB_T4POST, s.N);
+        items = outer * inner * Lt;
+      }
+      add_line_kernel(which, lp, items, cd, s.out_buf);
+    }
+  }
+};
+
+// ----------------------------------------------------- program building
+struct Shape {
+  std::vector<int64_t> d;  // dims with the batch count prepended
+};
+
+int64_t prod(const std::vector<int64_t>& v, size_t b, size_t e) {
+  int64_t p = 1;
+  for (size_t i = b; i < e; ++i) p *= v[i];
+  return p;
+}
+
+bool build_program(minfft_aux* a, int op, int howmany, bool alias, Program* prog) {
+  DeviceInfo di = device_info(a->device);
+  Planner pl{a, prog, di.max_smem, di.sms};
+  // full shape with the batch count as a leading, untransformed axis
+  std::vector<int64_t> D;
+  D.push_back(howmany);
+  for (int n : a->dims) D.push_back(n);
+  const size_t nd = D.size();  // >= 2
+  const bool multi = (nd > 2) || howmany > 1;
+
+  auto complex_axes = [&](std::vector<int64_t> shape, size_t first, size_t last_excl, int flags, int in_buf,
+                          int out_buf, bool reverse) {
+    // complex DFT along axes [first, last_excl) of `shape`
+    int cur = in_buf;
+    std::vector<size_t> order;
+    for (size_t ax = first; ax < last_excl; ++ax) order.push_back(ax);
+    if (reverse) std::reverse(order.begin(), order.end());
+    for (size_t ax : order) {
+      AxisStep s{};
+      s.combo = mb::K_CPLX;
+      s.N = shape[ax];
+      s.outer = prod(shape, 0, ax);
+      s.inner = prod(shape, ax + 1, shape.size());
+      s.in_row = s.N * s.inner;
+      s.out_row = s.in_row;
+      s.flags = flags;
+      s.in_buf = cur;
+      s.out_buf = out_buf;
+      pl.plan_axis(s);
+      if (!(s.N == 1 && cur == out_buf)) cur = out_buf;
+    }
+    return cur;
+  };
+
+  switch (op) {
+    case MINFFT_B200_DFT:
+    case MINFFT_B200_INVDFT: {
+      const int fl = (op == MINFFT_B200_INVDFT) ? (mb::F_CONJ_IN | mb::F_CONJ_OUT) : 0;
+      int cur = complex_axes(D, 1, nd, fl, BUF_X, BUF_Y, true);
+      if (cur != BUF_Y) pl.add_unit(mb::UNIT_COPY_CPLX, prod(D, 0, nd), 1, cur, BUF_Y);
+      break;
+    }
+    case MINFFT_B200_REALDFT: {
+      const int64_t N = D[nd - 1], K = N / 2 + 1;
+      const bool via_t1 = alias && multi;
+      std::vector<int64_t> H(D);
+      H[nd - 1] = K;
+      const size_t spec_bytes = size_t(prod(H, 0, nd)) * sizeof(cpx);
+      AxisStep s{};
+      s.combo = mb::K_R2C;
+      s.N = N;
+      s.outer = prod(D, 0, nd - 1);
+      s.inner = 1;
+      s.in_row = N;
+      s.out_row = K;
+      s.in_buf = BUF_X;
+      s.out_buf = via_t1 ? BUF_T1 : BUF_Y;
+      if (via_t1) pl.need(BUF_T1, spec_bytes);
+      pl.plan_axis(s);
+      int cur = complex_axes(H, 1, nd - 1, 0, s.out_buf, BUF_Y, true);
+      if (cur != BUF_Y) pl.add_unit(mb::UNIT_COPY_CPLX, prod(H, 0, nd), 1, cur, BUF_Y);
+      break;
+    }
+    case MINFFT_B200_INVREALDFT: {
+      const int64_t N = D[nd - 1], K = N / 2 + 1;
+      std::vector<int64_t> H(D);
+      H[nd - 1] = K;
+      const size_t spec_bytes = size_t(prod(H, 0, nd)) * sizeof(cpx);
+      int src = BUF_X;
+      if (nd > 2) {
+        pl.need(BUF_T1, spec_bytes);
+        src = complex_axes(H, 1, nd - 1, mb::F_CONJ_IN | mb::F_CONJ_OUT, BUF_X, BUF_T1, false);
+      }
+      const bool via_t1 = alias && howmany > 1 && nd == 2;
+      AxisStep s{};
+      s.combo = mb::K_C2R;
+      s.N = N;
+      s.outer = prod(D, 0, nd - 1);
+      s.inner = 1;
+      s.in_row = K;
+      s.out_row = N;
+      s.in_buf = src;
+      s.out_buf = via_t1 ? BUF_T1 : BUF_Y;
+      if (via_t1) pl.need(BUF_T1, size_t(prod(D, 0, nd)) * sizeof(real));
+      pl.plan_axis(s);
+      if (via_t1) pl.add_unit(mb::UNIT_SCALE_REAL, prod(D, 0, nd), 1, BUF_T1, BUF_Y);
+      break;
+    }
+    default: {
+      int combo = mb::K_T4, fl = 0;
+      if (op == MINFFT_B200_DCT2 || op == MINFFT_B200_DST2) combo = mb::K_DCT2;
+      if (op == MINFFT_B200_DCT3 || op == MINFFT_B200_DST3) combo = mb::K_DCT3;
+      if (op == MINFFT_B200_DST2 || op == MINFFT_B200_DST3 || op == MINFFT_B200_DST4) fl = mb::F_DST;
+      int cur = BUF_X;
+      for (size_t ax = nd - 1; ax >= 1; --ax) {
+        AxisStep s{};
+        s.combo = combo;
+        s.N = D[ax];
+        s.outer = prod(D, 0, ax);
+        s.inner = prod(D, ax + 1, nd);
+        s.in_row = s.N * s.inner;
+        s.out_row = s.in_row;
+        s.flags = fl;
+        s.in_buf = cur;
+        s.out_buf = BUF_Y;
+        pl.plan_axis(s);
+        if (!(s.N == 1 && combo == mb::K_DCT3 && cur == BUF_Y)) cur = BUF_Y;
+      }
+      if (cur != BUF_Y) pl.add_unit(mb::UNIT_SCALE_REAL, prod(D, 0, nd), 1, cur, BUF_Y);
+      break;
+    }
+  }
+  return pl.ok;
+}
+
+// bytes of one input / output array of op for plan a
+int64_t io_bytes(const minfft_aux* a, int op, bool output) {
+  const int64_t p = a->total;
+  const int64_t N = a->dims.back();
+  const int64_t spec = (p / N) * (N / 2 + 1);
+  switch (op) {
+    case MINFFT_B200_DFT:
+    case MINFFT_B200_INVDFT: return p * (int64_t)sizeof(cpx);
+    case MINFFT_B200_REALDFT: return output ? spec * (int64_t)sizeof(cpx) : p * (int64_t)sizeof(real);
+    case MINFFT_B200_INVREALDFT: return output ? p * (int64_t)sizeof(real) : spec * (int64_t)sizeof(cpx);
+    default: return p * (int64_t)sizeof(real);
+  }
+}
+
+bool ensure_buffer(minfft_aux* a, int buf, size_t bytes) {
+  if (bytes == 0 || a->buf_bytes[buf] >= bytes) return true;
+  if (a->bufs[buf]) cudaFree(a->bufs[buf]);
+  a->bufs[buf] = nullptr;
+  a->buf_bytes[buf] = 0;
+  void* p = nullptr;
+  if (!cuda_ok(cudaMalloc(&p, bytes), "cudaMalloc(scratch)")) return false;
+  a->bufs[buf] = p;
+  a->buf_bytes[buf] = bytes;
+  return true;
+}
+
+Program* get_program(minfft_aux* a, int op, int howmany, bool alias) {
+  auto key = std::make_tuple(op, howmany, alias ? 1 : 0);
+  auto it = a->programs.find(key);
+  if (it != a->programs.end()) return &it->second;
+  Program prog;
+  if (!build_program(a, op, howmany, alias, &prog)) return nullptr;
+  for (int b = BUF_T1; b < BUF_COUNT; ++b)
+    if (!ensure_buffer(a, b, prog.tbytes[b])) return nullptr;
+  return &(a->programs[key] = std::move(prog));
+}
+
+bool is_device_pointer(const void* p) {
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+bool run_program(minfft_aux* a, Program* prog, void* x, void* y) {
+  void* bufs[BUF_COUNT];
+  bufs[BUF_X] = x;
+  bufs[BUF_Y] = y;
+  for (int b = BUF_T1; b < BUF_COUNT; ++b) bufs[b] = a->bufs[b];
+  // complex data is accessed as aligned float2/double2: reject user buffers
+  // that are not, before anything is launched
+  for (const Launch& ln : prog->launches) {
+    const bool bad_in = ln.in_c && (reinterpret_cast<uintptr_t>(bufs[ln.in_buf]) % sizeof(cpx)) != 0;
+    const bool bad_out = ln.out_c && (reinterpret_cast<uintptr_t>(bufs[ln.out_buf]) % sizeof(cpx)) != 0;
+    if (bad_in || bad_out) {
+      set_error(MINFFT_B200_EINVAL, "complex data must be aligned to %zu bytes", sizeof(cpx));
+      return false;
+    }
+  }
+  for (Launch& ln : prog->launches) {
+    void* args[1];
+    size_t ev0 = 0;
+    if (a->prof) {
+      while (a->ev_pool.size() < a->ev_used + 2) {
+        cudaEvent_t e;
+        if (!cuda_ok(cudaEventCreate(&e), "cudaEventCreate")) return false;
+        a->ev_pool.push_back(e);
+      }
+      ev0 = a->ev_used;
+      a->ev_used += 2;
+      if (!cuda_ok(cudaEventRecord(a->ev_pool[ev0], a->stream), "cudaEventRecord")) return false;
+    }
+    if (ln.is_line) {
+      LineParams lp = ln.lp;
+      lp.in = bufs[ln.in_buf];
+      lp.out = bufs[ln.out_buf];
+      args[0] = &lp;
+      if (!cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, 0, a->stream), "launch(line)"))
+        return false;
+    } else {
+      AxisParams ap = ln.ap;
+      ap.in = bufs[ln.in_buf];
+      ap.out = bufs[ln.out_buf];
+      if (ln.vec_in && (reinterpret_cast<uintptr_t>(ap.in) % sizeof(cpx)) == 0) ap.flags |= mb::F_VEC;
+      if (ln.vec_out && (reinterpret_cast<uintptr_t>(ap.out) % sizeof(cpx)) == 0) ap.flags |= mb::F_VEC;
+      args[0] = &ap;
+      if (!cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, ln.smem, a->stream),
+                   "launch(axis)"))
+        return false;
+    }
+    if (a->prof) {
+      if (!cuda_ok(cudaEventRecord(a->ev_pool[ev0 + 1], a->stream), "cudaEventRecord")) return false;
+      a->pending.push_back({&ln, ev0, ev0 + 1});
+    }
+  }
+  return true;
+}
+
+// Fold recorded launch timings into the per-label statistics.
+bool harvest(minfft_aux* a) {
+  if (a->pending.empty()) return true;
+  if (!cuda_ok(cudaEventSynchronize(a->ev_pool[a->pending.back().e1]), "cudaEventSynchronize")) return false;
+  for (const auto& pe : a->pending) {
+    float ms = 0;
+    if (!cuda_ok(cudaEventElapsedTime(&ms, a->ev_pool[pe.e0], a->ev_pool[pe.e1]), "cudaEventElapsedTime"))
+      return false;
+    auto it = std::find_if(a->stats.begin(), a->stats.end(),
+                           [&](const minfft_aux::Stat& st) { return st.label == pe.ln->label; });
+    if (it == a->stats.end()) {
+      a->stats.push_back(minfft_aux::Stat());
+      it = a->stats.end() - 1;
+      it->label = pe.ln->label;
+      it->bytes = pe.ln->bytes;
+    }
+    it->launches += 1;
+    it->ms += ms;
+  }
+  a->pending.clear();
+  a->ev_used = 0;
+  return true;
+}
+
+bool grow(void** p, size_t* have, size_t want) {
+  if (*have >= want) return true;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  if (!cuda_ok(cudaMalloc(p, want), "cudaMalloc(staging)")) return false;
+  *have = want;
+  return true;
+}
+
+int execute(int op, void* x, void* y, int howmany, const minfft_aux* ca) {
+  minfft_aux* a = const_cast<minfft_aux*>(ca);
+  if (!a) {
+    set_error(MINFFT_B200_EINVAL, "NULL plan");
+    return MINFFT_B200_EINVAL;
+  }
+  if (op_family(op) != a->family) {
+    set_error(MINFFT_B200_EINVAL, "transform %d does not match the plan kind %d", op, a->family);
+    return MINFFT_B200_EINVAL;
+  }
+  if (!x || !y || howmany < 1) {
+    set_error(MINFFT_B200_EINVAL, "NULL data pointer or howmany < 1");
+    return MINFFT_B200_EINVAL;
+  }
+  DeviceGuard guard(a->device);
+  const size_t in_b = size_t(io_bytes(a, op, false)) * howmany;
+  const size_t out_b = size_t(io_bytes(a, op, true)) * howmany;
+  const bool x_dev = is_device_pointer(x), y_dev = is_device_pointer(y);
+  void* dx = x;
+  void* dy = y;
+  const bool same = (x == y);
+  if (!x_dev) {
+    if (!grow(&a->stage_in, &a->stage_in_bytes, std::max(in_b, same ? out_b : 0))) return g_err;
+    dx = a->stage_in;
+    if (!cuda_ok(cudaMemcpyAsync(dx, x, in_b, cudaMemcpyHostToDevice, a->stream), "cudaMemcpyAsync(H2D)"))
+      return g_err;
+  }
+  if (!y_dev) {
+    if (same) {
+      dy = dx;
+    } else {
+      if (!grow(&a->stage_out, &a->stage_out_bytes, out_b)) return g_err;
+      dy = a->stage_out;
+    }
+  }
+  const uintptr_t xs = reinterpret_cast<uintptr_t>(dx), ys = reinterpret_cast<uintptr_t>(dy);
+  const bool alias = (xs < ys + out_b) && (ys < xs + in_b);
+  Program* prog = get_program(a, op, howmany, alias);
+  if (!prog) return g_err ? g_err : MINFFT_B200_ECUDA;
+  if (!run_program(a, prog, dx, dy)) return g_err;
+  if (!y_dev) {
+    if (!cuda_ok(cudaMemcpyAsync(y, dy, out_b, cudaMemcpyDeviceToHost, a->stream), "cudaMemcpyAsync(D2H)"))
+      return g_err;
+    if (!cuda_ok(cudaStreamSynchronize(a->stream), "cudaStreamSynchronize")) return g_err;
+  }
+  return MINFFT_B200_OK;
+}
+
+// ---------------------------------------------------------------- makers
+minfft_aux* make_plan(int family, int d, const int* Ns) {
+  if (d < 1 || Ns == nullptr) {
+    set_error(MINFFT_B200_EINVAL, "dimension count must be >= 1");
+    return nullptr;
+  }
+  int64_t total = 1;
+  for (int i = 0; i < d; ++i) {
+    if (!is_pow2(Ns[i])) {
+      set_error(MINFFT_B200_EINVAL, "length %d is not a positive power of two", Ns[i]);
+      return nullptr;
+    }
+    total *= Ns[i];
+  }
+  if (total > (int64_t(1) << 31)) {
+    set_error(MINFFT_B200_EINVAL, "transform size exceeds 2^31 elements");
+    return nullptr;
+  }
+  minfft_aux* a = new (std::nothrow) minfft_aux();
+  if (!a) {
+    set_error(MINFFT_B200_ENOMEM, "host allocation failed");
+    return nullptr;
+  }
+  a->family = family;
+  a->dims.assign(Ns, Ns + d);
+  a->total = total;
+  if (!cuda_ok(cudaGetDevice(&a->device), "cudaGetDevice")) {
+    delete a;
+    return nullptr;
+  }
+  // plan every transform of the family (out of place, one array) now, so
+  // tables and scratch are allocated up front as the reference's makers do
+  static const int fam_ops[4][4] = {{MINFFT_B200_DFT, MINFFT_B200_INVDFT, -1, -1},
+                                    {MINFFT_B200_REALDFT, MINFFT_B200_INVREALDFT, -1, -1},
+                                    {MINFFT_B200_DCT2, MINFFT_B200_DST2, MINFFT_B200_DCT3, MINFFT_B200_DST3},
+                                    {MINFFT_B200_DCT4, MINFFT_B200_DST4, -1, -1}};
+  for (int k = 0; k < 4; ++k) {
+    const int op = fam_ops[family][k];
+    if (op < 0) continue;
+    if (!get_program(a, op, 1, false)) {
+      minfft_free_aux(a);
+      return nullptr;
+    }
+  }
+  return a;
+}
+
+}  // namespace
+
+// ===================================================================== ABI
+MB_EXPORT void minfft_free_aux(minfft_aux* a) {
+  if (!a) return;
+  {
+    DeviceGuard guard(a->device);
+    for (auto& kv : a->tables) cudaFree(kv.second);
+    for (int b = 0; b < BUF_COUNT; ++b)
+      if (a->bufs[b]) cudaFree(a->bufs[b]);
+    if (a->stage_in) cudaFree(a->stage_in);
+    if (a->stage_out) cudaFree(a->stage_out);
+    for (cudaEvent_t e : a->ev_pool) cudaEventDestroy(e);
+  }
+  delete a;
+}
+
+#define MB_TRANSFORM(name, code, TI, TO)                                   \
+  MB_EXPORT void minfft_##name(TI* x, TO* y, const minfft_aux* a) {       \
+    execute(code, static_cast<void*>(x), static_cast<void*>(y), 1, a);    \
+  }
+
+MB_TRANSFORM(dft, MINFFT_B200_DFT, minfft_cmpl, minfft_cmpl)
+MB_TRANSFORM(invdft, MINFFT_B200_INVDFT, minfft_cmpl, minfft_cmpl)
+MB_TRANSFORM(realdft, MINFFT_B200_REALDFT, minfft_real, minfft_cmpl)
+MB_TRANSFORM(invrealdft, MINFFT_B200_INVREALDFT, minfft_cmpl, minfft_real)
+MB_TRANSFORM(dct2, MINFFT_B200_DCT2, minfft_real, minfft_real)
+MB_TRANSFORM(dst2, MINFFT_B200_DST2, minfft_real, minfft_real)
+MB_TRANSFORM(dct3, MINFFT_B200_DCT3, minfft_real, minfft_real)
+MB_TRANSFORM(dst3, MINFFT_B200_DST3, minfft_real, minfft_real)
+MB_TRANSFORM(dct4, MINFFT_B200_DCT4, minfft_real, minfft_real)
+MB_TRANSFORM(dst4, MINFFT_B200_DST4, minfft_real, minfft_real)
+
+#define MB_MAKERS(fam, code)                                                                      \
+  MB_EXPORT minfft_aux* minfft_mkaux_##fam(int d, int* Ns) { return make_plan(code, d, Ns); }    \
+  MB_EXPORT minfft_aux* minfft_mkaux_##fam##_1d(int N) { return make_plan(code, 1, &N); }        \
+  MB_EXPORT minfft_aux* minfft_mkaux_##fam##_2d(int N1, int N2) {                                 \
+    int Ns[2] = {N1, N2};                                                                         \
+    return make_plan(code, 2, Ns);                                                                \
+  }                                                                                               \
+  MB_EXPORT minfft_aux* minfft_mkaux_##fam##_3d(int N1, int N2, int N3) {                         \
+    int Ns[3] = {N1, N2, N3};                                                                     \
+    return make_plan(code, 3, Ns);                                                                \
+  }
+
+MB_MAKERS(dft, FAM_DFT)
+MB_MAKERS(realdft, FAM_REALDFT)
+MB_MAKERS(t2t3, FAM_T2T3)
+MB_MAKERS(t4, FAM_T4)
+
+// ------------------------------------------------------------ extensions
+MB_EXPORT int minfft_b200_last_error(void) {
+  const int e = g_err;
+  g_err = 0;
+  return e;
+}
+
+MB_EXPORT const char* minfft_b200_last_error_message(void) { return g_msg; }
+
+MB_EXPORT int minfft_b200_set_stream(minfft_aux* a, void* stream) {
+  if (!a) {
+    set_error(MINFFT_B200_EINVAL, "NULL plan");
+    return MINFFT_B200_EINVAL;
+  }
+  a->stream = static_cast<cudaStream_t>(stream);
+  return MINFFT_B200_OK;
+}
+
+MB_EXPORT void* minfft_b200_get_stream(const minfft_aux* a) { return a ? static_cast<void*>(a->stream) : nullptr; }
+
+MB_EXPORT int minfft_b200_synchronize(const minfft_aux* a) {
+  if (!a) {
+    set_error(MINFFT_B200_EINVAL, "NULL plan");
+    return MINFFT_B200_EINVAL;
+  }
+  DeviceGuard guard(a->device);
+  return cuda_ok(cudaStreamSynchronize(a->stream), "cudaStreamSynchronize") ? MINFFT_B200_OK : g_err;
+}
+
+MB_EXPORT int minfft_b200_execute_batch(int op, void* x, void* y, int howmany, const minfft_aux* a) {
+  return execute(op, x, y, howmany, a);
+}
+
+MB_EXPORT long long minfft_b200_input_bytes(int op, const minfft_aux* a) {
+  if (!a || op_family(op) != a->family) return -1;
+  return io_bytes(a, op, false);
+}
+
+MB_EXPORT long long minfft_b200_output_bytes(int op, const minfft_aux* a) {
+  if (!a || op_family(op) != a->family) return -1;
+  return io_bytes(a, op, true);
+}
+
+MB_EXPORT long long minfft_b200_plan_bytes(const minfft_aux* a) {
+  if (!a) return -1;
+  long long b = (long long)a->table_bytes;
+  for (int i = 0; i < BUF_COUNT; ++i) b += (long long)a->buf_bytes[i];
+  return b;
+}
+
+MB_EXPORT int minfft_b200_launch_count(int op, const minfft_aux* ca) {
+  minfft_aux* a = const_cast<minfft_aux*>(ca);
+  if (!a || op_family(op) != a->family) return -1;
+  DeviceGuard guard(a->device);
+  Program* p = get_program(a, op, 1, false);
+  return p ? (int)p->launches.size() : -1;
+}
+
+MB_EXPORT int minfft_b200_profile(minfft_aux* a, int enable) {
+  if (!a) {
+    set_error(MINFFT_B200_EINVAL, "NULL plan");
+    return MINFFT_B200_EINVAL;
+  }
+  DeviceGuard guard(a->device);
+  if (!harvest(a)) return g_err;
+  a->prof = enable != 0;
+  a->stats.clear();
+  // enable > 1 reserves events for that many launches up front, so event
+  // creation stays out of a timed region
+  while (enable > 1 && a->ev_pool.size() < size_t(2) * size_t(enable)) {
+    cudaEvent_t e;
+    if (!cuda_ok(cudaEventCreate(&e), "cudaEventCreate")) return g_err;
+    a->ev_pool.push_back(e);
+  }
+  return MINFFT_B200_OK;
+}
+
+MB_EXPORT int minfft_b200_profile_count(minfft_aux* a) {
+  if (!a) return -1;
+  DeviceGuard guard(a->device);
+  if (!harvest(a)) return -1;
+  return (int)a->stats.size();
+}
+
+MB_EXPORT int minfft_b200_profile_entry(minfft_aux* a, int i, const char** label, long long* launches,
+                                        double* total_ms, double* bytes_per_launch) {
+  if (!a) return MINFFT_B200_EINVAL;
+  DeviceGuard guard(a->device);
+  if (!harvest(a)) return g_err;
+  if (i < 0 || i >= (int)a->stats.size()) return MINFFT_B200_EINVAL;
+  const auto& st = a->stats[i];
+  if (label) *label = st.label.c_str();
+  if (launches) *launches = st.launches;
+  if (total_ms) *total_ms = st.ms;
+  if (bytes_per_launch) *bytes_per_launch = st.bytes;
+  return MINFFT_B200_OK;
+}
