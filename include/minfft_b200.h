@@ -87,6 +87,17 @@ int minfft_b200_profile_count(minfft_aux *a);
 int minfft_b200_profile_entry(minfft_aux *a, int i, const char **label, long long *launches, double *total_ms,
                               double *bytes_per_launch);
 
+/* ------------------------------------------------------------ self-check */
+/* Plan transform `op` for dims Ns[0..d-1] (times `howmany` arrays; `alias`
+ * = input and output share memory) on the host only -- no device needed --
+ * and verify every planned kernel launch: the elements it reads and writes
+ * stay inside their buffers, launch shapes and shared memory are within
+ * limits, and passes that cannot run in place do not.  Returns the number of
+ * violations (0 = sound, -1 = bad arguments); `report` receives a
+ * description, `launches` the launch count. */
+int minfft_b200_plan_selfcheck(int op, int d, const int *Ns, int howmany, int alias, char *report, int report_len,
+                               int *launches);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -70,6 +70,9 @@ class Engine(MinfftLibrary):
         L.minfft_b200_profile_entry.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(i64),
                                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.minfft_b200_profile_entry.restype = i32
+        L.minfft_b200_plan_selfcheck.argtypes = [i32, i32, ctypes.POINTER(i32), i32, i32, ctypes.c_char_p, i32,
+                                                 ctypes.POINTER(i32)]
+        L.minfft_b200_plan_selfcheck.restype = i32
 
     # --------------------------------------------------------- errors
     def last_error(self) -> int:
@@ -104,6 +107,15 @@ class Engine(MinfftLibrary):
 
     def plan_bytes(self, aux: int) -> int:
         return int(self.lib.minfft_b200_plan_bytes(ctypes.c_void_p(aux)))
+
+    def plan_selfcheck(self, op: str, dims: Sequence[int], howmany: int = 1, alias: bool = False):
+        """Host-only planning check (no device): (violations, report, launch count)."""
+        arr = (ctypes.c_int * len(dims))(*[int(d) for d in dims])
+        buf = ctypes.create_string_buffer(4096)
+        n = ctypes.c_int(0)
+        bad = self.lib.minfft_b200_plan_selfcheck(OP_CODES[op], len(dims), arr, int(howmany), int(alias), buf, 4096,
+                                                  ctypes.byref(n))
+        return int(bad), buf.value.decode(), int(n.value)
 
     def profile(self, aux: int, enable: int) -> None:
         if self.lib.minfft_b200_profile(ctypes.c_void_p(aux), int(enable)):

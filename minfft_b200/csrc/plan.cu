@@ -69,20 +69,23 @@ bool cuda_ok(cudaError_t e, const char* what) {
 // (cos, sin)(2*pi*n/N), with the angle folded into [0, pi/4] before calling
 // libm -- the folding of reference minfft.c:989-1018, evaluated in double
 // for both precisions so the single-precision tables are correctly rounded.
+// The tests are written as 2n >= N, 4n >= N, 8n > N: identical to the
+// reference's n >= N/2, n >= N/4, n > N/8 for N >= 8, and still terminating
+// for N = 1, 2, 4 (where N/4 or N/8 would be 0).
 void unit_root(int64_t n, int64_t N, double* c, double* s) {
   if (n < 0) {
     unit_root(-n, N, c, s);
     *s = -*s;
-  } else if (n >= N / 2) {
+  } else if (2 * n >= N) {
     unit_root(n - N / 2, N, c, s);
     *c = -*c;
     *s = -*s;
-  } else if (n >= N / 4) {
+  } else if (4 * n >= N) {
     double cc, ss;
     unit_root(n - N / 4, N, &cc, &ss);
     *c = -ss;
     *s = cc;
-  } else if (n > N / 8) {
+  } else if (8 * n > N) {
     double cc, ss;
     unit_root(N / 4 - n, N, &cc, &ss);
     *c = ss;
@@ -115,7 +118,7 @@ bool is_pow2(int64_t v) { return v > 0 && (v & (v - 1)) == 0; }
 
 // =================================================== device properties
 struct DeviceInfo {
-  int max_smem = 48 * 1024;
+  int max_smem = 227 * 1024;  // B200 opt-in limit; replaced by the queried value
   int sms = 148;
 };
 
@@ -127,8 +130,16 @@ DeviceInfo device_info(int dev) {
   if (it != cache.end()) return it->second;
   DeviceInfo d;
   int v = 0;
-  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && v > 0) d.max_smem = v;
-  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0) d.sms = v;
+  if (dev >= 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && v > 0)
+      d.max_smem = v;
+    else
+      cudaGetLastError();
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+      d.sms = v;
+    else
+      cudaGetLastError();
+  }
   cache[dev] = d;
   return d;
 }
@@ -160,6 +171,9 @@ struct Launch {
   bool vec_out = false;  // same for the real output
   bool in_c = false;     // the kernel reads its input as complex values
   bool out_c = false;    // the kernel writes its output as complex values
+  bool hbm_pass = false; // a pass of the Stockham FFT over HBM (never in place)
+  int combo = -1;        // axis kernels: mb::Combo; line kernels: mb::LineKernel
+  int L = 0;             // axis kernels: in-CTA DFT length
   AxisParams ap;
   LineParams lp;
   std::string label;  // kernel and shape, for launch-level timing
@@ -210,6 +224,7 @@ struct minfft_aux {
   void* stage_out = nullptr;
   size_t stage_out_bytes = 0;
   size_t table_bytes = 0;
+  bool host_only = false;  // plan without a device (minfft_b200_plan_selfcheck)
   // launch-level timing (minfft_b200_profile)
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -237,6 +252,12 @@ const cpx* table(minfft_aux* a, int kind, int64_t N) {
   auto key = std::make_pair(kind, N);
   auto it = a->tables.find(key);
   if (it != a->tables.end()) return static_cast<const cpx*>(it->second);
+  if (a->host_only) {
+    // placeholder address: self-check plans are never executed
+    static cpx dummy[1];
+    a->tables[key] = dummy;
+    return dummy;
+  }
   std::vector<cpx> h;
   switch (kind) {
     case TB_TW:  // w_N^m, m < N
@@ -350,7 +371,7 @@ struct Planner {
       ok = false;
       return;
     }
-    if (!ensure_smem_attr(ln.fn, ln.smem)) {
+    if (!a->host_only && !ensure_smem_attr(ln.fn, ln.smem)) {
       ok = false;
       return;
     }
@@ -363,6 +384,8 @@ struct Planner {
     ln.vec_out = vec_out;
     ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R);
     ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C);
+    ln.combo = combo;
+    ln.L = L;
     ln.ap = ap;
     {
       static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4"};
@@ -392,6 +415,7 @@ struct Planner {
     ln.grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(sms) * 32)));
     ln.in_buf = in_buf;
     ln.out_buf = out_buf;
+    ln.combo = which;
     switch (which) {
       case mb::LK_C2R_PACK:
       case mb::LK_R2C_UNPACK: ln.in_c = ln.out_c = true; break;
@@ -620,6 +644,7 @@ struct Planner {
       if (last && conj_chain && s.combo != mb::K_DCT3) ap.flags |= mb::F_CONJ_OUT;
       ap.tw = tab(TB_TW, Rp);
       add_axis_kernel(mb::K_CPLX, (int)Rp, outer * (Lp / Rp), ap, prev, dst, false, false);
+      if (ok) prog->launches.back().hbm_pass = true;
       last_src = prev;
       prev = dst;
       Ns *= Rp;
@@ -809,8 +834,9 @@ Program* get_program(minfft_aux* a, int op, int howmany, bool alias) {
   if (it != a->programs.end()) return &it->second;
   Program prog;
   if (!build_program(a, op, howmany, alias, &prog)) return nullptr;
-  for (int b = BUF_T1; b < BUF_COUNT; ++b)
-    if (!ensure_buffer(a, b, prog.tbytes[b])) return nullptr;
+  if (!a->host_only)
+    for (int b = BUF_T1; b < BUF_COUNT; ++b)
+      if (!ensure_buffer(a, b, prog.tbytes[b])) return nullptr;
   return &(a->programs[key] = std::move(prog));
 }
 
@@ -1163,4 +1189,132 @@ MB_EXPORT int minfft_b200_profile_entry(minfft_aux* a, int i, const char** label
   if (total_ms) *total_ms = st.ms;
   if (bytes_per_launch) *bytes_per_launch = st.bytes;
   return MINFFT_B200_OK;
+}
+
+// ---------------------------------------------------------------- self-check
+namespace {
+
+struct Extent {
+  int64_t in_max, out_max;  // largest element index touched, in the buffer's element type
+};
+
+// Largest batch offset of an axis launch (all strides are non-negative).
+void axis_batch_max(const AxisParams& ap, int64_t& oi, int64_t& oo) {
+  const int64_t nb = ap.nbatch;
+  const int64_t b0 = std::min<int64_t>(ap.d0, nb) - 1;
+  const int64_t b1 = std::min<int64_t>(ap.d1, (nb + ap.d0 - 1) / ap.d0) - 1;
+  const int64_t b2 = (nb - 1) / (ap.d0 * ap.d1);
+  oi = b0 * ap.is0 + b1 * ap.is1 + b2 * ap.is2;
+  oo = b0 * ap.os0 + b1 * ap.os1 + b2 * ap.os2;
+}
+
+Extent launch_extent(const Launch& ln) {
+  Extent e{0, 0};
+  if (!ln.is_line) {
+    const AxisParams& ap = ln.ap;
+    const int64_t L = ln.L;
+    int64_t oi, oo;
+    axis_batch_max(ap, oi, oo);
+    switch (ln.combo) {
+      case mb::K_CPLX:
+        e.in_max = oi + (L - 1) * ap.in_n;
+        e.out_max = oo + (L - 1) * ap.out_k;
+        break;
+      case mb::K_R2C:
+        e.in_max = oi + 2 * L - 1;
+        e.out_max = oo + L * ap.out_k;
+        break;
+      case mb::K_C2R:
+        e.in_max = oi + L * ap.in_n;
+        e.out_max = oo + 2 * L - 1;
+        break;
+      default:
+        e.in_max = oi + (2 * L - 1) * ap.in_n;
+        e.out_max = oo + (2 * L - 1) * ap.out_k;
+        break;
+    }
+    return e;
+  }
+  const LineParams& lp = ln.lp;
+  const int64_t L = lp.L;
+  if (ln.combo == mb::LK_UNIT) {
+    e.in_max = e.out_max = L - 1;
+    return e;
+  }
+  int64_t in_n = 0, out_n = 0;
+  switch (ln.combo) {
+    case mb::LK_DCT2_PRE:
+    case mb::LK_T4_PRE:
+    case mb::LK_DCT3_PACK: in_n = 2 * L - 1; out_n = L - 1; break;
+    case mb::LK_C2R_PACK: in_n = L; out_n = L - 1; break;
+    case mb::LK_R2C_UNPACK: in_n = L - 1; out_n = L; break;
+    default: in_n = L - 1; out_n = 2 * L - 1; break;
+  }
+  e.in_max = (lp.outer - 1) * lp.in_so + in_n * lp.in_sn + (lp.inner - 1);
+  e.out_max = (lp.outer - 1) * lp.out_so + out_n * lp.out_sn + (lp.inner - 1);
+  return e;
+}
+
+}  // namespace
+
+// Plan `op` for the given shape without touching a device and check every
+// launch: element ranges inside their buffers, complex/real views of the
+// user buffers, launch shapes, and no in-place use of the passes that
+// cannot run in place.  Returns the number of violations (0 = plan is
+// sound); a description of the first ones goes to `report`.
+MB_EXPORT int minfft_b200_plan_selfcheck(int op, int d, const int* Ns, int howmany, int alias, char* report,
+                                         int report_len, int* launches) {
+  const int fam = op_family(op);
+  std::string rep;
+  if (fam < 0 || d < 1 || !Ns || howmany < 1) return -1;
+  for (int i = 0; i < d; ++i)
+    if (!is_pow2(Ns[i])) return -1;
+  minfft_aux a;
+  a.family = fam;
+  a.dims.assign(Ns, Ns + d);
+  a.total = 1;
+  for (int i = 0; i < d; ++i) a.total *= Ns[i];
+  a.device = -1;
+  a.host_only = true;
+  Program prog;
+  if (!build_program(&a, op, howmany, alias != 0, &prog)) {
+    if (report && report_len > 0) snprintf(report, report_len, "planning failed: %s", g_msg);
+    return 1;
+  }
+  int bad = 0;
+  auto fail = [&](const char* fmt, auto... args) {
+    ++bad;
+    char buf[256];
+    snprintf(buf, sizeof(buf), fmt, args...);
+    if (rep.size() < 2000) rep += std::string(buf) + "\n";
+  };
+  size_t cap[BUF_COUNT];
+  cap[BUF_X] = size_t(io_bytes(&a, op, false)) * howmany;
+  cap[BUF_Y] = size_t(io_bytes(&a, op, true)) * howmany;
+  if (alias) cap[BUF_X] = cap[BUF_Y] = std::max(cap[BUF_X], cap[BUF_Y]);
+  for (int b = BUF_T1; b < BUF_COUNT; ++b) cap[b] = prog.tbytes[b];
+  const DeviceInfo di = device_info(-1);
+  for (size_t i = 0; i < prog.launches.size(); ++i) {
+    const Launch& ln = prog.launches[i];
+    const Extent e = launch_extent(ln);
+    const size_t ie = ln.in_c ? sizeof(cpx) : sizeof(real), oe = ln.out_c ? sizeof(cpx) : sizeof(real);
+    if (size_t(e.in_max + 1) * ie > cap[ln.in_buf])
+      fail("launch %zu (%s): input reaches byte %lld of buffer %d (%zu bytes)", i, ln.label.c_str(),
+           (long long)((e.in_max + 1) * ie), ln.in_buf, cap[ln.in_buf]);
+    if (size_t(e.out_max + 1) * oe > cap[ln.out_buf])
+      fail("launch %zu (%s): output reaches byte %lld of buffer %d (%zu bytes)", i, ln.label.c_str(),
+           (long long)((e.out_max + 1) * oe), ln.out_buf, cap[ln.out_buf]);
+    if (ln.block < 1 || ln.block > 1024 || ln.grid < 1) fail("launch %zu: bad shape %u x %u", i, ln.grid, ln.block);
+    if (!ln.is_line && ln.block > 512) fail("launch %zu: block %u above launch bounds", i, ln.block);
+    if (ln.smem > size_t(di.max_smem)) fail("launch %zu: %zu bytes of shared memory", i, ln.smem);
+    const bool alias_io = (ln.in_buf == ln.out_buf) || (alias && ((ln.in_buf == BUF_X && ln.out_buf == BUF_Y) ||
+                                                                 (ln.in_buf == BUF_Y && ln.out_buf == BUF_X)));
+    if (alias_io && (ln.hbm_pass || (ln.is_line && ln.combo != mb::LK_UNIT)))
+      fail("launch %zu (%s): runs in place but cannot", i, ln.label.c_str());
+    if (!ln.is_line && ln.grid > 0 && int64_t(ln.grid) * ln.ap.cpb < ln.ap.nbatch)
+      fail("launch %zu: grid does not cover the batch", i);
+  }
+  if (launches) *launches = (int)prog.launches.size();
+  if (report && report_len > 0) snprintf(report, report_len, "%s", rep.c_str());
+  return bad;
 }

@@ -64,7 +64,9 @@ static cpx c_ipos(cpx a) { return c_make(-a.im, a.re); }
 /* ------------------------------------------------------------------ */
 /* unit roots: (cos, sin)(2*pi*n/N) with the angle folded into the    */
 /* first octant before libm is called (minfft.c:989-1018).  The       */
-/* angle 2*pi*n/N is formed in the working precision, as there.       */
+/* angle 2*pi*n/N is formed in the working precision, as there.  The  */
+/* folding tests 2n >= N, 4n >= N, 8n > N equal the reference's for   */
+/* N >= 8 and also terminate for N < 8.                               */
 /* ------------------------------------------------------------------ */
 
 static cpx unit_root(long n, long N)
@@ -76,20 +78,20 @@ static cpx unit_root(long n, long N)
         r.im = -r.im;
         return r;
     }
-    if (n >= N / 2) {                  /* rotate by pi */
+    if (2 * n >= N) {                  /* rotate by pi */
         r = unit_root(n - N / 2, N);
         r.re = -r.re;
         r.im = -r.im;
         return r;
     }
-    if (n >= N / 4) {                  /* rotate by pi/2 */
+    if (4 * n >= N) {                  /* rotate by pi/2 */
         r = unit_root(n - N / 4, N);
         s = r.re;
         r.re = -r.im;
         r.im = s;
         return r;
     }
-    if (n > N / 8) {                   /* reflect about pi/4 */
+    if (8 * n > N) {                   /* reflect about pi/4 */
         r = unit_root(N / 4 - n, N);
         s = r.re;
         r.re = r.im;

@@ -1,0 +1,62 @@
+"""Planner soundness on the CPU: every launch the engine would enqueue for a
+shape stays inside its buffers, uses valid launch shapes, and never runs a
+pass in place that cannot run in place.  This is the host-side reading of
+the kernels' index arithmetic, done for every workload size before any of it
+runs on a GPU."""
+import itertools
+
+import numpy as np
+import pytest
+
+import minfft_b200
+from minfft_b200 import OPS
+
+SHAPES = [(1,), (2,), (4,), (8,), (16,), (32,), (64,), (128,), (256,), (512,), (1024,), (2048,), (4096,), (8192,),
+          (16384,), (32768,), (65536,), (1 << 17), (1 << 20), (4, 8), (16, 32), (1, 8), (8, 1), (64, 128), (2, 4, 8),
+          (8, 16, 4), (2, 1, 4), (1, 2, 1), (2, 2, 4, 8), (32, 32, 32), (8192, 4), (4, 8192), (2, 16384), (16384, 2),
+          (8, 8, 8192), (2048, 2048), (256, 256, 256), (1, 1, 1, 1, 2), (2, 8192, 2)]
+SHAPES = [s if isinstance(s, tuple) else (s,) for s in SHAPES]
+HUGE = [(1 << 26,), (1 << 24,), (1 << 22,), (4096, 4096), (16, 1 << 16)]
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["double", "single"])
+@pytest.mark.parametrize("dims", SHAPES, ids=lambda d: "x".join(map(str, d)))
+def test_plans_are_in_bounds(dims, single):
+    eng = minfft_b200.engine(single)
+    for op in OPS:
+        for howmany, alias in itertools.product((1, 3), (False, True)):
+            bad, rep, n = eng.plan_selfcheck(op, dims, howmany, alias)
+            assert bad == 0, f"{op} {dims} howmany={howmany} alias={alias}:\n{rep}"
+            assert n >= 1 or (op in ("dft", "invdft", "dct3", "dst3") and int(np.prod(dims)) == 1 and alias)
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["double", "single"])
+@pytest.mark.parametrize("dims", HUGE, ids=lambda d: "x".join(map(str, d)))
+def test_workload_plans_are_in_bounds(dims, single):
+    eng = minfft_b200.engine(single)
+    for op in OPS:
+        for alias in (False, True):
+            bad, rep, _ = eng.plan_selfcheck(op, dims, 1, alias)
+            assert bad == 0, f"{op} {dims} alias={alias}:\n{rep}"
+
+
+def test_batched_4096_plan_is_one_launch_per_direction():
+    eng = minfft_b200.engine(False)
+    for op in ("dft", "invdft"):
+        bad, rep, n = eng.plan_selfcheck(op, (4096,), 1024, False)
+        assert bad == 0 and n == 1, rep
+
+
+def test_2d_workload_launch_counts():
+    """2048 x 2048: one fused row kernel and one column kernel per transform."""
+    for single in (False, True):
+        eng = minfft_b200.engine(single)
+        for op in ("realdft", "invrealdft", "dct2", "dct3"):
+            bad, rep, n = eng.plan_selfcheck(op, (2048, 2048), 1, False)
+            assert bad == 0 and n == 2, (op, n, rep)
+
+
+def test_selfcheck_rejects_bad_arguments():
+    eng = minfft_b200.engine(False)
+    assert eng.plan_selfcheck("dft", (12,))[0] == -1
+    assert eng.plan_selfcheck("dft", (8,), howmany=0)[0] == -1
