@@ -50,7 +50,7 @@ __host__ __device__ constexpr double kCos32(int q) {
          : q == 3 ? 0.831469612302545237078788377617905756
          : q == 4 ? 0.707106781186547524400844362104849039
          : q == 5 ? 0.555570233019602224742830813948532874
-         : q == 6 ? 0.382683432536089771731266804398316950
+         : q == 6 ? 0.382683432365089771728459984030398867
          : q == 7 ? 0.195090322016128267848284868477022240
                   : 0.0;
 }

@@ -88,3 +88,15 @@ def test_engine_refuses_to_load_without_library(tmp_path, monkeypatch):
     monkeypatch.setitem(minfft_b200.LIB_PATHS, False, str(tmp_path / "nope.so"))
     with pytest.raises(ImportError):
         minfft_b200.Engine(False)
+
+
+def test_compile_time_root_constants_are_exact():
+    """The in-register butterflies use literal cos(pi*q/16) constants; check
+    every literal against a 40-digit evaluation."""
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.dps = 40
+    src = open(os.path.join(ROOT, "minfft_b200", "csrc", "common.cuh")).read()
+    vals = re.findall(r"q == (\d) \? ([0-9.]+)", src)
+    assert len(vals) == 7
+    for q, v in vals:
+        assert abs(mpmath.mpf(v) - mpmath.cos(mpmath.pi * int(q) / 16)) < 1e-30, (q, v)
