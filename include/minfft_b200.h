@@ -87,6 +87,23 @@ int minfft_b200_profile_count(minfft_aux *a);
 int minfft_b200_profile_entry(minfft_aux *a, int i, const char **label, long long *launches, double *total_ms,
                               double *bytes_per_launch);
 
+/* ------------------------------------------------- allocation-free DFT */
+/* No counterpart in the reference.  Complex DFT (inverse = 0) or unnormalised
+ * inverse DFT (inverse != 0) of length n, a power of two in [4, 262144],
+ * from device array x to device array y (complex values of this library's
+ * precision; x == y allowed), enqueued on `stream` (NULL: the legacy default
+ * stream).  It allocates nothing: for callers that cannot call cudaMalloc
+ * -- device memory owned by another allocator's pool, fixed memory budgets,
+ * loops where an allocation's latency and implied synchronisation are not
+ * acceptable -- and so cannot hold a plan.  Its scratch (4 MiB double /
+ * 2 MiB single, plus the call's root tables) is a static device array that
+ * every GPU loading the library keeps until exit; all calls share it, so
+ * calls that overlap on the GPU race and must be ordered by the caller.  The
+ * first call on each device looks up the array's address; make it before
+ * any stream capture.  Lengths outside the range return MINFFT_B200_EINVAL
+ * with nothing launched. */
+int minfft_b200_dft_noalloc(const void *x, void *y, int n, int inverse, void *stream);
+
 /* ------------------------------------------------------------ self-check */
 /* Plan transform `op` for dims Ns[0..d-1] (times `howmany` arrays; `alias`
  * = input and output share memory) on the host only -- no device needed --

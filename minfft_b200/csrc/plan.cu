@@ -58,6 +58,15 @@ void set_error(int code, const char* fmt, ...) {
   va_end(ap);
 }
 
+}  // namespace
+
+namespace mb {
+// Records a failure for minfft_b200_last_error() (used by other translation units).
+void set_last_error(int code, const char* msg) { set_error(code, "%s", msg); }
+}  // namespace mb
+
+namespace {
+
 bool cuda_ok(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return true;
   set_error(e == cudaErrorMemoryAllocation ? MINFFT_B200_ENOMEM : MINFFT_B200_ECUDA, "%s: %s", what,
