@@ -87,6 +87,41 @@ __device__ __forceinline__ void batch_offsets(const AxisParams& p, int64_t b, in
 }
 
 // ------------------------------------------------------------ Stockham core
+// u[r] *= w^r for r = 1..RP-1 with w = tw[i1]: two table roots (w, w^4) per
+// sub-DFT, the other powers formed just before use as products of at most
+// four roundings, so only a handful of roots are live at a time.
+template <int RP>
+__device__ __forceinline__ void apply_root_powers(cpx* u, const cpx* __restrict__ tw, int i1) {
+  static_assert(RP <= 16, "radix up to 16");
+  const cpx w1 = ldg(tw + i1);
+  u[1] = cmul(u[1], w1);
+  if constexpr (RP > 2) {
+    const cpx w2 = cmul(w1, w1);
+    u[2] = cmul(u[2], w2);
+    const cpx w3 = cmul(w2, w1);
+    u[3] = cmul(u[3], w3);
+    if constexpr (RP > 4) {
+      const cpx w4 = ldg(tw + 4 * i1);
+      u[4] = cmul(u[4], w4);
+      u[5] = cmul(u[5], cmul(w4, w1));
+      u[6] = cmul(u[6], cmul(w4, w2));
+      u[7] = cmul(u[7], cmul(w4, w3));
+      if constexpr (RP > 8) {
+        const cpx w8 = cmul(w4, w4);
+        u[8] = cmul(u[8], w8);
+        u[9] = cmul(u[9], cmul(w8, w1));
+        u[10] = cmul(u[10], cmul(w8, w2));
+        u[11] = cmul(u[11], cmul(w8, w3));
+        const cpx w12 = cmul(w8, w4);
+        u[12] = cmul(u[12], w12);
+        u[13] = cmul(u[13], cmul(w12, w1));
+        u[14] = cmul(u[14], cmul(w12, w2));
+        u[15] = cmul(u[15], cmul(w12, w3));
+      }
+    }
+  }
+}
+
 template <int L, int R, int RP, int NS>
 __device__ __forceinline__ void pass_compute(cpx (&v)[R], int j, const cpx* __restrict__ tw) {
   constexpr int S = R / RP;  // sub-DFTs per thread in this pass
@@ -99,8 +134,7 @@ __device__ __forceinline__ void pass_compute(cpx (&v)[R], int j, const cpx* __re
       const int jp = j + s * (L / R);
       const int q = jp & (NS - 1);
       constexpr int step = L / (NS * RP);
-#pragma unroll
-      for (int r = 1; r < RP; ++r) u[r] = cmul(u[r], ldg(tw + q * r * step));
+      apply_root_powers<RP>(u, tw, q * step);
     }
     fft_reg<RP>(u);
 #pragma unroll
@@ -158,7 +192,7 @@ struct LoadCplx {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int64_t n = x.j + r * (L / R);
-      v[r] = x.active ? in[n * p.in_n] : czero();
+      v[r] = x.active ? __ldcs(in + n * p.in_n) : czero();
     }
     if (p.flags & F_CONJ_IN) {
 #pragma unroll
@@ -194,7 +228,7 @@ struct LoadR2C {
       if (!x.active)
         v[r] = czero();
       else if (vec)
-        v[r] = reinterpret_cast<const cpx*>(in)[n];
+        v[r] = __ldcs(reinterpret_cast<const cpx*>(in) + n);
       else
         v[r] = cmk(in[2 * n], in[2 * n + 1]);
     }
@@ -542,8 +576,17 @@ struct RadixFor {
   static constexpr int value = L >= 16 ? 16 : L;
 };
 
+// Register budget: 512 threads x 2 CTAs (64 registers) in single precision,
+// 512 x 1 (128 registers) in double, where each thread holds 16 complex
+// doubles.
+#if MINFFT_SINGLE
+constexpr int kMinBlocks = 2;
+#else
+constexpr int kMinBlocks = 1;
+#endif
+
 template <int L, class LoadOp, class StoreOp>
-__global__ void __launch_bounds__(512) axis_pass_kernel(const AxisParams p) {
+__global__ void __launch_bounds__(512, kMinBlocks) axis_pass_kernel(const AxisParams p) {
   constexpr int R = RadixFor<L>::value;
   constexpr int TPT = L / R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
