@@ -239,6 +239,9 @@ class WorkloadBatch4096:
     def plans(self):
         yield self.eng, self.plan, ("dft", "invdft")
 
+    def howmany_for(self, op):
+        return self.howmany
+
     def step(self, k):
         x = self.xs[k % self.nsets]
         self.plan.batch("dft", x.data_ptr(), self.y.data_ptr(), self.howmany)
@@ -370,6 +373,13 @@ def run_engine(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
     W = WORKLOADS[args.workload](torch, dev)
+    tuned = 0
+    if not args.no_tune:
+        # project autotuner: pick kernel form and tile size per launch (setup, untimed)
+        for eng, plan, ops in W.plans():
+            for op in ops:
+                eng.autotune(plan.aux, op, getattr(W, "howmany_for", lambda o: 1)(op), 5)
+            tuned = max(tuned, eng.tune_size())
     launches_per_step = W.launches_per_step()
 
     # warm-up
@@ -476,6 +486,7 @@ def run_engine(args):
                 "vs_baseline": None, "dtype": "f64+f32" if args.workload == "2d2048" else "f64",
                 "data": "synthetic", "config": W.config(), "parallelism": f"replicas x{world}",
                 "gpu_launches": int(launches_per_step * args.steps), "clocks": clocks.summary(),
+                "autotuned_launch_configs": tuned,
                 "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "kernels": kernel_table[:8]}
         print(json.dumps(line))
     if dist:
@@ -493,6 +504,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="2d2048")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (heuristic launch configurations)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -104,6 +104,24 @@ int minfft_b200_profile_entry(minfft_aux *a, int i, const char **label, long lon
  * with nothing launched. */
 int minfft_b200_dft_noalloc(const void *x, void *y, int n, int inverse, void *stream);
 
+/* ------------------------------------------------------------- autotuner */
+/* Time the candidate launch configurations (kernel form: one tile per CTA
+ * or persistent CTAs with double-buffered asynchronous copies; transforms per
+ * CTA) of every kernel launch of transform `op` on `howmany` arrays of plan
+ * `a`, using scratch buffers (`reps` timed runs each), and keep the fastest
+ * in a process-wide table that every plan consults when it builds its launch
+ * lists.  The table can be saved to and loaded from a text file. */
+int minfft_b200_autotune(minfft_aux *a, int op, int howmany, int reps);
+int minfft_b200_tune_save(const char *path);
+int minfft_b200_tune_load(const char *path);
+int minfft_b200_tune_clear(void);
+int minfft_b200_tune_size(void);
+/* Configuration for launches without a table entry: pipe = 1 persistent
+ * pipelined kernels, 0 one tile per CTA, -1 the planner's heuristic; cpb > 0
+ * transforms per CTA (reduced until it fits), 0 the heuristic.  Applies to
+ * plans built afterwards. */
+int minfft_b200_tune_set_default(int pipe, int cpb);
+
 /* ------------------------------------------------------------ self-check */
 /* Plan transform `op` for dims Ns[0..d-1] (times `howmany` arrays; `alias`
  * = input and output share memory) on the host only -- no device needed --

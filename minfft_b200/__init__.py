@@ -73,6 +73,17 @@ class Engine(MinfftLibrary):
         L.minfft_b200_plan_selfcheck.argtypes = [i32, i32, ctypes.POINTER(i32), i32, i32, ctypes.c_char_p, i32,
                                                  ctypes.POINTER(i32)]
         L.minfft_b200_plan_selfcheck.restype = i32
+        L.minfft_b200_autotune.argtypes = [vp, i32, i32, i32]
+        L.minfft_b200_autotune.restype = i32
+        for f in ("minfft_b200_tune_save", "minfft_b200_tune_load"):
+            getattr(L, f).argtypes = [ctypes.c_char_p]
+            getattr(L, f).restype = i32
+        L.minfft_b200_tune_clear.argtypes = []
+        L.minfft_b200_tune_clear.restype = i32
+        L.minfft_b200_tune_size.argtypes = []
+        L.minfft_b200_tune_size.restype = i32
+        L.minfft_b200_tune_set_default.argtypes = [i32, i32]
+        L.minfft_b200_tune_set_default.restype = i32
 
     # --------------------------------------------------------- errors
     def last_error(self) -> int:
@@ -116,6 +127,29 @@ class Engine(MinfftLibrary):
         bad = self.lib.minfft_b200_plan_selfcheck(OP_CODES[op], len(dims), arr, int(howmany), int(alias), buf, 4096,
                                                   ctypes.byref(n))
         return int(bad), buf.value.decode(), int(n.value)
+
+    def autotune(self, aux: int, op: str, howmany: int = 1, reps: int = 5) -> None:
+        """Tune every launch of `op` on this plan (kernel form, tile size) on the device."""
+        if self.lib.minfft_b200_autotune(ctypes.c_void_p(aux), OP_CODES[op], int(howmany), int(reps)):
+            self.check()
+
+    def tune_save(self, path: str) -> None:
+        if self.lib.minfft_b200_tune_save(path.encode()):
+            self.check()
+
+    def tune_load(self, path: str) -> None:
+        if self.lib.minfft_b200_tune_load(path.encode()):
+            self.check()
+
+    def tune_clear(self) -> None:
+        self.lib.minfft_b200_tune_clear()
+
+    def tune_size(self) -> int:
+        return int(self.lib.minfft_b200_tune_size())
+
+    def tune_set_default(self, pipe: int = -1, cpb: int = 0) -> None:
+        """Launch configuration where the tuning table has no entry (-1/0: planner's choice)."""
+        self.lib.minfft_b200_tune_set_default(int(pipe), int(cpb))
 
     def profile(self, aux: int, enable: int) -> None:
         if self.lib.minfft_b200_profile(ctypes.c_void_p(aux), int(enable)):

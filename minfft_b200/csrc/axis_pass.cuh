@@ -44,9 +44,13 @@ struct AxisParams {
   int64_t st_div;    // elements per span index (product of trailing dims)
   int st_shift;      // log2(Lt / (st_ns * L))
   int st_lobits;
-  int cpb;      // transforms per CTA
+  int cpb;      // transforms per CTA (per tile in the pipelined kernel)
   int colmode;  // 1: thread index runs fastest over the transform
   int flags;
+  int chunk;    // pipelined kernel: bytes per asynchronous copy (16, 8 or 4)
+  int64_t ntiles;       // pipelined kernel: number of tiles
+  int64_t gpb;          // pipelined kernel, column mode: tiles per d0 block
+  int stage_bytes;      // pipelined kernel: bytes of one shared-memory stage
   int pad_;
 };
 
@@ -348,16 +352,21 @@ struct LoadC2R {
 // t1 = w_4N^n (n < N/2), t2 = w_N^k (k < L/2); N = 2L.
 struct LoadDCT3 {
   static constexpr bool kStaged = true;
-  static __device__ __forceinline__ cpx zval(const real* in, int64_t s, int n, int L, bool dst, const cpx* e) {
+  // z_n of the type-3 pre-rotation; rd(i) returns input real x_i
+  template <class Rd>
+  static __device__ __forceinline__ cpx zval_r(const Rd& rd, int n, int L, bool dst, const cpx* e) {
     const int N = 2 * L;
-    if (n == 0) return cmk(dst ? in[int64_t(N - 1) * s] : in[0], real(0));
+    if (n == 0) return cmk(dst ? rd(N - 1) : rd(0), real(0));
     if (n == L) {
       const real r2 = real(1.414213562373095048801688724209698079);
-      return cmk(r2 * (dst ? in[int64_t(L - 1) * s] : in[int64_t(L) * s]), real(0));
+      return cmk(r2 * (dst ? rd(L - 1) : rd(L)), real(0));
     }
-    const real a = dst ? in[int64_t(N - n - 1) * s] : in[int64_t(n) * s];
-    const real b = dst ? in[int64_t(n - 1) * s] : in[int64_t(N - n) * s];
+    const real a = dst ? rd(N - n - 1) : rd(n);
+    const real b = dst ? rd(n - 1) : rd(N - n);
     return cconj(cmul(cmk(a, b), ldg(e + n)));
+  }
+  static __device__ __forceinline__ cpx zval(const real* in, int64_t s, int n, int L, bool dst, const cpx* e) {
+    return zval_r([&](int i) { return in[int64_t(i) * s]; }, n, L, dst, e);
   }
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
@@ -394,6 +403,7 @@ struct LoadDCT3 {
 struct TileOffsets {
   int64_t* in_off;
   int64_t* out_off;
+  int nvalid;  // transforms of the tile that exist (the rest are padding)
 };
 
 struct StoreCplx {
@@ -417,11 +427,9 @@ struct StoreCplx {
     __syncthreads();
     scatter_natural<L, R>(v, x.j, x.c, t);
     __syncthreads();
-    const int total = p.cpb * L;
+    const int total = to.nvalid * L;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       const int c = e / L, k = e - c * L;
-      const int64_t b = int64_t(blockIdx.x) * p.cpb + c;
-      if (b >= p.nbatch) continue;
       cpx o = t.s[t.idx(c, k)];
       if (cj) o.y = -o.y;
       out[to.out_off[c] + int64_t(k) * p.out_k] = o;
@@ -591,7 +599,8 @@ __global__ void __launch_bounds__(512, kMinBlocks) axis_pass_kernel(const AxisPa
   constexpr int TPT = L / R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   int64_t* offs = reinterpret_cast<int64_t*>(smem_raw);
-  TileOffsets to{offs, offs + p.cpb};
+  const int64_t left = p.nbatch - int64_t(blockIdx.x) * p.cpb;
+  TileOffsets to{offs, offs + p.cpb, int(left < p.cpb ? left : p.cpb)};
   Tile t{reinterpret_cast<cpx*>(smem_raw + 16 * ((2 * p.cpb * sizeof(int64_t) + 15) / 16)), p.cpb, p.colmode,
          padded_len(L)};
 

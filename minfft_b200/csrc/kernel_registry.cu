@@ -3,6 +3,8 @@
 // they compile in parallel.
 #include "kernel_registry.h"
 
+#include "common.cuh"
+
 namespace mb {
 
 const void* axis_kernel_cplx(int log2L);
@@ -11,6 +13,37 @@ const void* axis_kernel_c2r(int log2L);
 const void* axis_kernel_dct2(int log2L);
 const void* axis_kernel_dct3(int log2L);
 const void* axis_kernel_t4(int log2L);
+
+const void* pipe_kernel_cplx(int log2L);
+const void* pipe_kernel_r2c(int log2L);
+const void* pipe_kernel_c2r(int log2L);
+const void* pipe_kernel_dct2(int log2L);
+const void* pipe_kernel_dct3(int log2L);
+const void* pipe_kernel_t4(int log2L);
+
+const void* pipe_kernel(int combo, int log2L) {
+  switch (combo) {
+    case K_CPLX: return pipe_kernel_cplx(log2L);
+    case K_R2C: return pipe_kernel_r2c(log2L);
+    case K_C2R: return pipe_kernel_c2r(log2L);
+    case K_DCT2: return pipe_kernel_dct2(log2L);
+    case K_DCT3: return pipe_kernel_dct3(log2L);
+    case K_T4: return pipe_kernel_t4(log2L);
+    default: return nullptr;
+  }
+}
+
+int pipe_raw_size(int combo) {
+  return (combo == K_CPLX || combo == K_C2R) ? int(sizeof(cpx)) : int(sizeof(real));
+}
+
+int pipe_raw_elems(int combo, int L) {
+  switch (combo) {
+    case K_CPLX: return L;
+    case K_C2R: return L + 1;
+    default: return 2 * L;
+  }
+}
 
 const void* axis_kernel(int combo, int log2L) {
   switch (combo) {

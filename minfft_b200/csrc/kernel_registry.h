@@ -19,4 +19,13 @@ constexpr int kMaxLog2L = 13;  // largest in-CTA DFT: 8192 points
 // Returns the kernel function for combo and log2(L), or nullptr.
 const void* axis_kernel(int combo, int log2L);
 
+// The persistent, software-pipelined form of the same kernels (pipe_pass.cuh),
+// for log2(L) = 1 .. 13, or nullptr.
+const void* pipe_kernel(int combo, int log2L);
+
+// Raw input element size and raw elements per transform of the pipelined
+// kernel of `combo` (complex or real input, L, L+1 or 2L elements).
+int pipe_raw_size(int combo);
+int pipe_raw_elems(int combo, int L);
+
 }  // namespace mb

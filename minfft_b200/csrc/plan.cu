@@ -29,10 +29,12 @@
 #include <new>
 #include <set>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "axis_pass.cuh"
 #include "kernel_registry.h"
+#include "pipe_pass.cuh"
 #include "line_kernels.h"
 #include "minfft.h"
 #include "minfft_b200.h"
@@ -167,6 +169,45 @@ bool ensure_smem_attr(const void* fn, size_t bytes) {
   return true;
 }
 
+// ------------------------------------------------------------- autotuning
+// Launch configuration of an axis pass: kernel form and transforms per CTA
+// (per tile for the pipelined form).  The autotuner (minfft_b200_autotune)
+// times the candidates of each launch of a plan on the device and records
+// the fastest here, keyed by everything that shapes the launch; the planner
+// consults this table before falling back to its heuristics.
+struct TuneKey {
+  int combo, L, colmode, hbm, staged;
+  int64_t nbatch, d0, in_n, out_k;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(combo, L, colmode, hbm, staged, nbatch, d0, in_n, out_k) <
+           std::tie(o.combo, o.L, o.colmode, o.hbm, o.staged, o.nbatch, o.d0, o.in_n, o.out_k);
+  }
+};
+struct TuneVal {
+  int pipe;
+  int cpb;
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+TuneVal g_default_override{-1, 0};  // minfft_b200_tune_set_default: form (-1 = heuristic) and tile
+thread_local const std::map<TuneKey, TuneVal>* t_force = nullptr;  // candidates under test
+
+bool tune_lookup(const TuneKey& k, TuneVal* v) {
+  if (t_force) {
+    auto it = t_force->find(k);
+    if (it != t_force->end()) {
+      *v = it->second;
+      return true;
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(k);
+  if (it == g_tune.end()) return false;
+  *v = it->second;
+  return true;
+}
+
 // ============================================================ programs
 enum Buf : int { BUF_X = 0, BUF_Y, BUF_T1, BUF_T2, BUF_T3, BUF_T4, BUF_COUNT };
 
@@ -181,7 +222,10 @@ struct Launch {
   bool in_c = false;     // the kernel reads its input as complex values
   bool out_c = false;    // the kernel writes its output as complex values
   bool hbm_pass = false; // a pass of the Stockham FFT over HBM (never in place)
+  bool pipe = false;     // persistent pipelined kernel (pipe_pass.cuh)
+  int ch_static = 16;    // pipelined kernel: copy chunk allowed by the strides
   int combo = -1;        // axis kernels: mb::Combo; line kernels: mb::LineKernel
+  TuneKey key{};         // axis kernels: autotuning key
   int L = 0;             // axis kernels: in-CTA DFT length
   AxisParams ap;
   LineParams lp;
@@ -361,10 +405,72 @@ struct Planner {
     return combo == mb::K_R2C || combo == mb::K_C2R || combo == mb::K_DCT2 || combo == mb::K_DCT3;
   }
 
+  // default kernel form when no tuned configuration exists (the pipelined
+  // form is chosen per launch by the autotuner; MINFFT_B200_PIPE=1 makes it
+  // the default)
+  static bool pipe_default() {
+    static const bool on = [] {
+      const char* e = getenv("MINFFT_B200_PIPE");
+      return e && e[0] == '1';
+    }();
+    return on;
+  }
+
+  int max_threads_cpb(int L) const { return std::max(1, 512 / (L / std::min(16, L))); }
+
+  // largest power of two <= 16 dividing every value
+  static int pow2_align(std::initializer_list<int64_t> vals) {
+    int a = 16;
+    for (int64_t v : vals)
+      while (a > 4 && (v % a) != 0) a /= 2;
+    return a;
+  }
+
+  bool pipe_fits(int combo, int L, int cpb) const {
+    return L >= 2 && mb::pipe_kernel(combo, ilog2(L)) && cpb >= 1 && cpb <= max_threads_cpb(L) &&
+           mb::pipe_smem(L, cpb, mb::pipe_raw_elems(combo, L), mb::pipe_raw_size(combo)) <= (size_t)dev_max_smem;
+  }
+
+  bool plain_fits(int combo, int L, int cpb, int flags) const {
+    const bool tile = (L > std::min(16, L)) || staged(combo) || (flags & mb::F_STAGE_ROWS);
+    const size_t sm = tile ? mb::axis_pass_smem(L, cpb) : size_t(16 * ((2 * cpb * sizeof(int64_t) + 15) / 16));
+    return cpb >= 1 && cpb <= max_threads_cpb(L) && sm <= (size_t)dev_max_smem;
+  }
+
   void add_axis_kernel(int combo, int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, bool vec_in,
                        bool vec_out) {
     const int lg = ilog2(L);
+    const TuneKey key{combo, L, ap.colmode, ap.st_ns > 1 ? 1 : 0, (ap.flags & mb::F_STAGE_ROWS) ? 1 : 0,
+                      nbatch, ap.d0, ap.in_n, ap.out_k};
+    TuneVal tv;
+    if (tune_lookup(key, &tv)) {
+      if (tv.pipe && pipe_fits(combo, L, tv.cpb)) {
+        add_pipe_kernel(combo, L, nbatch, ap, in_buf, out_buf, tv.cpb, key);
+        return;
+      }
+      if (!tv.pipe && plain_fits(combo, L, tv.cpb, ap.flags)) ap.cpb = tv.cpb;
+    } else {
+      TuneVal ov;
+      {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        ov = g_default_override;
+      }
+      const bool want_pipe = ov.pipe == 1 || (ov.pipe < 0 && pipe_default());
+      if (want_pipe) {
+        int pc = ov.cpb > 0 ? ov.cpb : choose_pipe_cpb(combo, L, ap.colmode != 0);
+        while (pc > 1 && !pipe_fits(combo, L, pc)) pc /= 2;
+        if (pipe_fits(combo, L, pc)) {
+          add_pipe_kernel(combo, L, nbatch, ap, in_buf, out_buf, pc, key);
+          return;
+        }
+      } else if (ov.pipe == 0 && ov.cpb > 0) {
+        int c = ov.cpb;
+        while (c > 1 && !plain_fits(combo, L, c, ap.flags)) c /= 2;
+        ap.cpb = c;
+      }
+    }
     Launch ln;
+    ln.key = key;
     ln.fn = mb::axis_kernel(combo, lg);
     if (!ln.fn) {
       set_error(MINFFT_B200_EUNSUPPORTED, "no kernel for combo %d, L=%d", combo, L);
@@ -409,6 +515,90 @@ struct Planner {
       ln.bytes = per * double(nbatch);
       char buf[160];
       snprintf(buf, sizeof(buf), "axis_pass<%s,L=%d,%s%s> batch=%lld", names[combo], L, ap.colmode ? "col" : "row",
+               ap.st_ns > 1 ? ",hbm" : "", (long long)nbatch);
+      ln.label = buf;
+    }
+    prog->launches.push_back(ln);
+  }
+
+  // transforms per tile of the pipelined kernel: two stages must fit
+  int choose_pipe_cpb(int combo, int L, bool colmode) {
+    const int R = std::min(16, L);
+    const int tpt = L / R;
+    int cpb = std::max(1, 256 / tpt);
+    if (colmode) {
+      const int want = int(64 / mb::pipe_raw_size(combo));  // 64-byte runs of adjacent columns
+      if (cpb < want) cpb = std::max(cpb, std::min(want, std::max(1, 512 / tpt)));
+    }
+    const int er = mb::pipe_raw_elems(combo, L);
+    while (cpb > 1 && mb::pipe_smem(L, cpb, er, mb::pipe_raw_size(combo)) > (size_t)dev_max_smem) cpb /= 2;
+    return cpb;
+  }
+
+  void add_pipe_kernel(int combo, int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, int cpb,
+                       const TuneKey& key) {
+    const int lg = ilog2(L);
+    Launch ln;
+    ln.key = key;
+    ln.fn = mb::pipe_kernel(combo, lg);
+    ln.pipe = true;
+    const int R = std::min(16, L);
+    const int tpt = L / R;
+    const int esz = mb::pipe_raw_size(combo), er = mb::pipe_raw_elems(combo, L);
+    ap.cpb = cpb;
+    ap.nbatch = nbatch;
+    if (ap.colmode) {
+      ap.gpb = (ap.d0 + ap.cpb - 1) / ap.cpb;
+      ap.ntiles = (nbatch / ap.d0) * ap.gpb;
+      ln.ch_static = pow2_align({int64_t(ap.cpb) * esz, ap.in_n * esz, ap.is1 * esz, ap.is2 * esz});
+    } else {
+      ap.gpb = 0;
+      ap.ntiles = (nbatch + ap.cpb - 1) / ap.cpb;
+      const int64_t run = int64_t(er % 2 == 1 ? er - 1 : er) * esz;
+      ln.ch_static = pow2_align({run, int64_t(er) * esz, ap.is1 * esz, ap.is2 * esz});
+    }
+    ap.stage_bytes = (int)mb::pipe_stage_bytes(L, ap.cpb, er, esz);
+    ln.smem = mb::pipe_smem(L, ap.cpb, er, esz);
+    if (ln.smem > (size_t)dev_max_smem) {
+      set_error(MINFFT_B200_EUNSUPPORTED, "shared memory %zu exceeds %d", ln.smem, dev_max_smem);
+      ok = false;
+      return;
+    }
+    if (!a->host_only && !ensure_smem_attr(ln.fn, ln.smem)) {
+      ok = false;
+      return;
+    }
+    ln.block = unsigned(ap.cpb * tpt);
+    int occ = 1;
+    if (!a->host_only) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ln.fn, (int)ln.block, ln.smem) != cudaSuccess ||
+          occ < 1) {
+        cudaGetLastError();
+        occ = 1;
+      }
+    }
+    ln.grid = unsigned(std::min<int64_t>(ap.ntiles, int64_t(sms) * occ));
+    ln.in_buf = in_buf;
+    ln.out_buf = out_buf;
+    ln.vec_out = (combo == mb::K_C2R);
+    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R);
+    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C);
+    ln.combo = combo;
+    ln.L = L;
+    ln.ap = ap;
+    {
+      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4"};
+      const double Rb = sizeof(real), C = sizeof(cpx);
+      double per = 0;
+      switch (combo) {
+        case mb::K_CPLX: per = 2.0 * L * C; break;
+        case mb::K_R2C: per = 2.0 * L * Rb + (L + 1) * C; break;
+        case mb::K_C2R: per = (L + 1) * C + 2.0 * L * Rb; break;
+        default: per = 4.0 * L * Rb; break;
+      }
+      ln.bytes = per * double(nbatch);
+      char buf[160];
+      snprintf(buf, sizeof(buf), "axis_pipe<%s,L=%d,%s%s> batch=%lld", names[combo], L, ap.colmode ? "col" : "row",
                ap.st_ns > 1 ? ",hbm" : "", (long long)nbatch);
       ln.label = buf;
     }
@@ -869,6 +1059,30 @@ struct DeviceGuard {
   }
 };
 
+// Enqueue one planned launch with its buffers resolved.
+bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
+  void* args[1];
+  if (ln.is_line) {
+    LineParams lp = ln.lp;
+    lp.in = bufs[ln.in_buf];
+    lp.out = bufs[ln.out_buf];
+    args[0] = &lp;
+    return cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, 0, a->stream), "launch(line)");
+  }
+  AxisParams ap = ln.ap;
+  ap.in = bufs[ln.in_buf];
+  ap.out = bufs[ln.out_buf];
+  if (ln.vec_in && (reinterpret_cast<uintptr_t>(ap.in) % sizeof(cpx)) == 0) ap.flags |= mb::F_VEC;
+  if (ln.vec_out && (reinterpret_cast<uintptr_t>(ap.out) % sizeof(cpx)) == 0) ap.flags |= mb::F_VEC;
+  if (ln.pipe) {
+    int ch = ln.ch_static;
+    while (ch > 4 && (reinterpret_cast<uintptr_t>(ap.in) % ch) != 0) ch /= 2;
+    ap.chunk = ch;
+  }
+  args[0] = &ap;
+  return cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, ln.smem, a->stream), "launch(axis)");
+}
+
 bool run_program(minfft_aux* a, Program* prog, void* x, void* y) {
   void* bufs[BUF_COUNT];
   bufs[BUF_X] = x;
@@ -885,7 +1099,6 @@ bool run_program(minfft_aux* a, Program* prog, void* x, void* y) {
     }
   }
   for (Launch& ln : prog->launches) {
-    void* args[1];
     size_t ev0 = 0;
     if (a->prof) {
       while (a->ev_pool.size() < a->ev_used + 2) {
@@ -897,24 +1110,7 @@ bool run_program(minfft_aux* a, Program* prog, void* x, void* y) {
       a->ev_used += 2;
       if (!cuda_ok(cudaEventRecord(a->ev_pool[ev0], a->stream), "cudaEventRecord")) return false;
     }
-    if (ln.is_line) {
-      LineParams lp = ln.lp;
-      lp.in = bufs[ln.in_buf];
-      lp.out = bufs[ln.out_buf];
-      args[0] = &lp;
-      if (!cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, 0, a->stream), "launch(line)"))
-        return false;
-    } else {
-      AxisParams ap = ln.ap;
-      ap.in = bufs[ln.in_buf];
-      ap.out = bufs[ln.out_buf];
-      if (ln.vec_in && (reinterpret_cast<uintptr_t>(ap.in) % sizeof(cpx)) == 0) ap.flags |= mb::F_VEC;
-      if (ln.vec_out && (reinterpret_cast<uintptr_t>(ap.out) % sizeof(cpx)) == 0) ap.flags |= mb::F_VEC;
-      args[0] = &ap;
-      if (!cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, ln.smem, a->stream),
-                   "launch(axis)"))
-        return false;
-    }
+    if (!launch_one(a, ln, bufs)) return false;
     if (a->prof) {
       if (!cuda_ok(cudaEventRecord(a->ev_pool[ev0 + 1], a->stream), "cudaEventRecord")) return false;
       a->pending.push_back({&ln, ev0, ev0 + 1});
@@ -1320,10 +1516,202 @@ MB_EXPORT int minfft_b200_plan_selfcheck(int op, int d, const int* Ns, int howma
                                                                  (ln.in_buf == BUF_Y && ln.out_buf == BUF_X)));
     if (alias_io && (ln.hbm_pass || (ln.is_line && ln.combo != mb::LK_UNIT)))
       fail("launch %zu (%s): runs in place but cannot", i, ln.label.c_str());
-    if (!ln.is_line && ln.grid > 0 && int64_t(ln.grid) * ln.ap.cpb < ln.ap.nbatch)
+    if (!ln.is_line && !ln.pipe && ln.grid > 0 && int64_t(ln.grid) * ln.ap.cpb < ln.ap.nbatch)
       fail("launch %zu: grid does not cover the batch", i);
+    if (ln.pipe) {
+      const AxisParams& ap = ln.ap;
+      if (ap.colmode) {
+        if (ap.nbatch % ap.d0 != 0) fail("launch %zu: column tiles would straddle d0 blocks", i);
+        if ((ap.nbatch / ap.d0) * ap.gpb != ap.ntiles || ap.gpb * ap.cpb < ap.d0)
+          fail("launch %zu: column tiles do not cover the batch", i);
+      } else {
+        if (ap.ntiles * ap.cpb < ap.nbatch) fail("launch %zu: row tiles do not cover the batch", i);
+        if (ap.in_n != 1 && ln.combo != mb::K_R2C) fail("launch %zu: row-mode copy needs contiguous rows", i);
+      }
+      if (ln.grid < 1 || int64_t(ln.grid) > ap.ntiles) fail("launch %zu: persistent grid %u", i, ln.grid);
+      const int esz = mb::pipe_raw_size(ln.combo);
+      if (ln.ch_static < esz && ln.ch_static < 16 && esz <= 16 && ln.ch_static % 4 != 0)
+        fail("launch %zu: copy chunk %d", i, ln.ch_static);
+      if (size_t(ap.stage_bytes) < size_t(ap.cpb) * mb::pipe_raw_elems(ln.combo, ln.L) * esz ||
+          size_t(ap.stage_bytes) < size_t(ap.cpb) * mb::padded_len(ln.L) * sizeof(cpx))
+        fail("launch %zu: stage of %d bytes too small", i, ap.stage_bytes);
+    }
   }
   if (launches) *launches = (int)prog.launches.size();
   if (report && report_len > 0) snprintf(report, report_len, "%s", rep.c_str());
   return bad;
+}
+
+// ------------------------------------------------------------- autotuner
+namespace {
+
+// Mean milliseconds of `reps` back-to-back runs of one launch (after one
+// untimed run), or a negative value on error.
+float time_launch(minfft_aux* a, const Launch& ln, void* const* bufs, int reps) {
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return -1;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return -1;
+  }
+  float ms = -1;
+  if (launch_one(a, ln, bufs) && cudaEventRecord(e0, a->stream) == cudaSuccess) {
+    bool ok = true;
+    for (int r = 0; r < reps && ok; ++r) ok = launch_one(a, ln, bufs);
+    if (ok && cudaEventRecord(e1, a->stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+      ms /= float(reps);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms;
+}
+
+}  // namespace
+
+// Time every candidate configuration (kernel form x transforms per CTA) of
+// each axis launch of transform `op` on `howmany` arrays, on scratch
+// buffers, and record the fastest in the process-wide tuning table; the
+// plan's launch lists are then rebuilt with the winners.  Returns 0 or an
+// error code.
+MB_EXPORT int minfft_b200_autotune(minfft_aux* a, int op, int howmany, int reps) {
+  if (!a || op_family(op) != a->family || howmany < 1) {
+    set_error(MINFFT_B200_EINVAL, "bad autotune arguments");
+    return MINFFT_B200_EINVAL;
+  }
+  if (reps < 1) reps = 5;
+  DeviceGuard guard(a->device);
+  if (!harvest(a)) return g_err;
+  Program* p0 = get_program(a, op, howmany, false);
+  if (!p0) return g_err ? g_err : MINFFT_B200_ECUDA;
+  std::vector<TuneKey> keys;
+  for (const Launch& ln : p0->launches)
+    if (!ln.is_line) keys.push_back(ln.key);
+  const size_t in_b = size_t(io_bytes(a, op, false)) * howmany, out_b = size_t(io_bytes(a, op, true)) * howmany;
+  void *x = nullptr, *y = nullptr;
+  if (!cuda_ok(cudaMalloc(&x, in_b), "cudaMalloc(autotune)")) return g_err;
+  if (!cuda_ok(cudaMalloc(&y, out_b), "cudaMalloc(autotune)")) {
+    cudaFree(x);
+    return g_err;
+  }
+  cudaMemsetAsync(x, 0, in_b, a->stream);
+  cudaMemsetAsync(y, 0, out_b, a->stream);
+  DeviceInfo di = device_info(a->device);
+  std::map<TuneKey, TuneVal> force, best;
+  t_force = &force;
+  int rc = MINFFT_B200_OK;
+  for (const TuneKey& key : keys) {
+    if (best.count(key)) continue;
+    Planner probe{a, nullptr, di.max_smem, di.sms};
+    float best_ms = 1e30f;
+    TuneVal best_v{0, 0};
+    for (int pipe = 0; pipe <= 1; ++pipe) {
+      for (int cpb = 1; cpb <= probe.max_threads_cpb(key.L); cpb *= 2) {
+        const bool fits = pipe ? probe.pipe_fits(key.combo, key.L, cpb)
+                               : probe.plain_fits(key.combo, key.L, cpb, key.staged ? mb::F_STAGE_ROWS : 0);
+        if (!fits) continue;
+        force[key] = TuneVal{pipe, cpb};
+        Program P;
+        if (!build_program(a, op, howmany, false, &P)) continue;
+        bool bufs_ok = true;
+        for (int b = BUF_T1; b < BUF_COUNT; ++b) bufs_ok &= ensure_buffer(a, b, P.tbytes[b]);
+        if (!bufs_ok) {
+          rc = g_err;
+          break;
+        }
+        void* bufs[BUF_COUNT] = {x, y, a->bufs[BUF_T1], a->bufs[BUF_T2], a->bufs[BUF_T3], a->bufs[BUF_T4]};
+        for (const Launch& ln : P.launches) {
+          if (ln.is_line || ln.key < key || key < ln.key) continue;
+          const float ms = time_launch(a, ln, bufs, reps);
+          if (ms > 0 && ms < best_ms) {
+            best_ms = ms;
+            best_v = TuneVal{pipe, cpb};
+          }
+          break;
+        }
+      }
+    }
+    force.erase(key);
+    if (best_ms < 1e29f) best[key] = best_v;
+  }
+  t_force = nullptr;
+  cudaStreamSynchronize(a->stream);
+  cudaGetLastError();
+  cudaFree(x);
+  cudaFree(y);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (auto& kv : best) g_tune[kv.first] = kv.second;
+  }
+  a->programs.clear();
+  return rc;
+}
+
+// Save / load / clear the process-wide tuning table (text, one entry per line).
+MB_EXPORT int minfft_b200_tune_save(const char* path) {
+  if (!path) return MINFFT_B200_EINVAL;
+  FILE* f = fopen(path, "w");
+  if (!f) {
+    set_error(MINFFT_B200_EINVAL, "cannot write %s", path);
+    return MINFFT_B200_EINVAL;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  fprintf(f, "# minfft_b200 tuning table (%s): combo L colmode hbm staged nbatch d0 in_n out_k pipe cpb\n",
+          sizeof(real) == 8 ? "double" : "single");
+  for (auto& kv : g_tune) {
+    const TuneKey& k = kv.first;
+    fprintf(f, "%d %d %d %d %d %lld %lld %lld %lld %d %d\n", k.combo, k.L, k.colmode, k.hbm, k.staged,
+            (long long)k.nbatch, (long long)k.d0, (long long)k.in_n, (long long)k.out_k, kv.second.pipe,
+            kv.second.cpb);
+  }
+  fclose(f);
+  return MINFFT_B200_OK;
+}
+
+MB_EXPORT int minfft_b200_tune_load(const char* path) {
+  if (!path) return MINFFT_B200_EINVAL;
+  FILE* f = fopen(path, "r");
+  if (!f) {
+    set_error(MINFFT_B200_EINVAL, "cannot read %s", path);
+    return MINFFT_B200_EINVAL;
+  }
+  char line[512];
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  while (fgets(line, sizeof(line), f)) {
+    if (line[0] == '#') continue;
+    TuneKey k{};
+    TuneVal v{};
+    long long nb, d0, in_n, out_k;
+    if (sscanf(line, "%d %d %d %d %d %lld %lld %lld %lld %d %d", &k.combo, &k.L, &k.colmode, &k.hbm, &k.staged, &nb,
+               &d0, &in_n, &out_k, &v.pipe, &v.cpb) == 11) {
+      k.nbatch = nb;
+      k.d0 = d0;
+      k.in_n = in_n;
+      k.out_k = out_k;
+      g_tune[k] = v;
+    }
+  }
+  fclose(f);
+  return MINFFT_B200_OK;
+}
+
+MB_EXPORT int minfft_b200_tune_clear(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.clear();
+  return MINFFT_B200_OK;
+}
+
+MB_EXPORT int minfft_b200_tune_size(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return (int)g_tune.size();
+}
+
+// Launch configuration used where the tuning table has no entry: pipe = 1
+// persistent pipelined kernels, 0 one tile per CTA, -1 the planner's choice;
+// cpb > 0 sets transforms per CTA (reduced until it fits), 0 the heuristic.
+// Plans built afterwards use it.
+MB_EXPORT int minfft_b200_tune_set_default(int pipe, int cpb) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_default_override = TuneVal{pipe < 0 ? -1 : (pipe ? 1 : 0), cpb < 0 ? 0 : cpb};
+  return MINFFT_B200_OK;
 }

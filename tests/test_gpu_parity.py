@@ -304,3 +304,49 @@ def test_config_large_t4_2_24(single):
         x = make_input(op, dims, rng, single)
         err = rel_l2(gpu_apply(op, x, dims, single), expected(op, x, dims))
         assert err <= tolerance(single, dims), (op, err)
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+def test_autotuned_plans_stay_correct(single, tmp_path):
+    """The autotuner may pick either kernel form and any tile size; every
+    choice must give the same results, and the table survives a save/load."""
+    eng = minfft_b200.engine(single)
+    rng = np.random.default_rng(41)
+    for dims in [(2048,), (64, 1024), (1024, 8), (1 << 15,)]:
+        for op in OPS:
+            x = make_input(op, dims, rng, single)
+            p = eng.plan(OP_FAMILY[op], dims)
+            eng.autotune(p.aux, op, 1, 2)
+            p.free()
+            err = rel_l2(gpu_apply(op, x, dims, single), expected(op, x, dims))
+            assert err <= tolerance(single, dims), (op, dims, err)
+    n = eng.tune_size()
+    assert n > 0
+    path = str(tmp_path / "tune.txt")
+    eng.tune_save(path)
+    eng.tune_clear()
+    assert eng.tune_size() == 0
+    eng.tune_load(path)
+    assert eng.tune_size() == n
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+@pytest.mark.parametrize("pipe", [0, 1], ids=["tile", "pipelined"])
+def test_every_forced_configuration_is_correct(single, pipe):
+    """Both kernel forms at every tile size (transforms per CTA), forced as the
+    default configuration, on row and column passes of every transform kind."""
+    eng = minfft_b200.engine(single)
+    rng = np.random.default_rng(43)
+    saved = eng.tune_size()
+    try:
+        eng.tune_clear()
+        for cpb in (1, 2, 4, 8, 16, 64):
+            eng.tune_set_default(pipe, cpb)
+            for dims in [(64, 512), (8, 2048), (1 << 14,)]:
+                for op in OPS:
+                    x = make_input(op, dims, rng, single)
+                    err = rel_l2(gpu_apply(op, x, dims, single), expected(op, x, dims))
+                    assert err <= tolerance(single, dims), (op, dims, cpb, err)
+    finally:
+        eng.tune_set_default(-1, 0)
+    assert saved >= 0

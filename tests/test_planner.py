@@ -60,3 +60,20 @@ def test_selfcheck_rejects_bad_arguments():
     eng = minfft_b200.engine(False)
     assert eng.plan_selfcheck("dft", (12,))[0] == -1
     assert eng.plan_selfcheck("dft", (8,), howmany=0)[0] == -1
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["double", "single"])
+@pytest.mark.parametrize("pipe", [0, 1], ids=["tile", "pipelined"])
+def test_every_launch_configuration_is_in_bounds(single, pipe):
+    """Every kernel form and tile size the autotuner may pick, on every shape."""
+    eng = minfft_b200.engine(single)
+    try:
+        for cpb in (1, 2, 4, 8, 16, 32, 64, 128, 256, 512):
+            eng.tune_set_default(pipe, cpb)
+            for dims in SHAPES + HUGE[:3]:
+                for op in OPS:
+                    for alias in (False, True):
+                        bad, rep, _ = eng.plan_selfcheck(op, dims, 2, alias)
+                        assert bad == 0, f"pipe={pipe} cpb={cpb} {op} {dims} alias={alias}:\n{rep}"
+    finally:
+        eng.tune_set_default(-1, 0)
