@@ -106,8 +106,8 @@ int minfft_b200_dft_noalloc(const void *x, void *y, int n, int inverse, void *st
 
 /* ------------------------------------------------------------- autotuner */
 /* Time the candidate launch configurations (kernel form: one tile per CTA
- * or persistent CTAs with double-buffered asynchronous copies; transforms per
- * CTA) of every kernel launch of transform `op` on `howmany` arrays of plan
+ * or persistent CTAs with double-buffered asynchronous copies; per-thread
+ * radix 8 or 16; transforms per CTA) of every kernel launch of transform `op` on `howmany` arrays of plan
  * `a`, using scratch buffers (`reps` timed runs each), and keep the fastest
  * in a process-wide table that every plan consults when it builds its launch
  * lists.  The table can be saved to and loaded from a text file. */
@@ -118,9 +118,9 @@ int minfft_b200_tune_clear(void);
 int minfft_b200_tune_size(void);
 /* Configuration for launches without a table entry: pipe = 1 persistent
  * pipelined kernels, 0 one tile per CTA, -1 the planner's heuristic; cpb > 0
- * transforms per CTA (reduced until it fits), 0 the heuristic.  Applies to
- * plans built afterwards. */
-int minfft_b200_tune_set_default(int pipe, int cpb);
+ * transforms per CTA (reduced until it fits), 0 the heuristic; radix 8 or 16
+ * complex values per thread.  Applies to plans built afterwards. */
+int minfft_b200_tune_set_default(int pipe, int cpb, int radix);
 
 /* ------------------------------------------------------------ self-check */
 /* Plan transform `op` for dims Ns[0..d-1] (times `howmany` arrays; `alias`

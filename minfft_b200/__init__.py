@@ -82,7 +82,7 @@ class Engine(MinfftLibrary):
         L.minfft_b200_tune_clear.restype = i32
         L.minfft_b200_tune_size.argtypes = []
         L.minfft_b200_tune_size.restype = i32
-        L.minfft_b200_tune_set_default.argtypes = [i32, i32]
+        L.minfft_b200_tune_set_default.argtypes = [i32, i32, i32]
         L.minfft_b200_tune_set_default.restype = i32
 
     # --------------------------------------------------------- errors
@@ -147,9 +147,9 @@ class Engine(MinfftLibrary):
     def tune_size(self) -> int:
         return int(self.lib.minfft_b200_tune_size())
 
-    def tune_set_default(self, pipe: int = -1, cpb: int = 0) -> None:
+    def tune_set_default(self, pipe: int = -1, cpb: int = 0, radix: int = 16) -> None:
         """Launch configuration where the tuning table has no entry (-1/0: planner's choice)."""
-        self.lib.minfft_b200_tune_set_default(int(pipe), int(cpb))
+        self.lib.minfft_b200_tune_set_default(int(pipe), int(cpb), int(radix))
 
     def profile(self, aux: int, enable: int) -> None:
         if self.lib.minfft_b200_profile(ctypes.c_void_p(aux), int(enable)):

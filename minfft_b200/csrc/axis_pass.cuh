@@ -51,7 +51,7 @@ struct AxisParams {
   int64_t ntiles;       // pipelined kernel: number of tiles
   int64_t gpb;          // pipelined kernel, column mode: tiles per d0 block
   int stage_bytes;      // pipelined kernel: bytes of one shared-memory stage
-  int pad_;
+  int lp;               // shared-memory pitch between transforms (tile_pitch)
 };
 
 enum : int {
@@ -62,15 +62,32 @@ enum : int {
   F_VEC = 16,         // real rows are aligned for paired (complex) vector access
 };
 
-// Shared-memory tile: cpb transforms of L complex values, padded every 16
-// elements so strided Stockham scatters spread over all banks.
+// Shared-memory tile: cpb transforms of L complex values, transform c at
+// c*lp, element p at pad16(p) (one spare slot every 16 elements, so strided
+// Stockham scatters spread over all banks).  The pitch lp is skewed by the
+// host (tile_pitch) so that the threads of one 128-byte wavefront -- several
+// short transforms in row mode, several adjacent columns in column mode --
+// land in distinct banks.
 struct Tile {
   cpx* s;
-  int cpb;
-  int colmode;
   int lp;
-  __device__ __forceinline__ int idx(int c, int p) const { return colmode ? pad16(p) * cpb + c : c * lp + pad16(p); }
+  __device__ __forceinline__ int idx(int c, int p) const { return c * lp + pad16(p); }
 };
+
+// Pitch (in complex elements) between the transforms of a tile.
+__host__ __device__ inline int tile_pitch(int L, int R, int cpb, int colmode) {
+  const int W = int(128 / sizeof(cpx));  // complex values per wavefront
+  const int tpt = L / (L < R ? L : R);
+  int target = 0;
+  if (colmode)
+    target = cpb >= W ? 1 : W / cpb;
+  else if (tpt < W)
+    target = tpt;
+  int lp = padded_len(L);
+  if (target > 0)
+    while (lp % W != target % W) ++lp;
+  return lp;
+}
 
 // Per-thread context: which transform, which thread within it, offsets.
 struct Ctx {
@@ -146,28 +163,47 @@ __device__ __forceinline__ void pass_compute(cpx (&v)[R], int j, const cpx* __re
   }
 }
 
+// Stockham scatter of a pass with span NS: element r of sub-DFT jp goes to
+// B + r*NS with B = (jp/NS)*NS*RP + jp%NS.  Either NS = 1 (B is a multiple of
+// RP and r < RP) or NS*RP >= 16 (the part of B above jp%NS is a multiple of
+// 16 and jp%NS < NS); in both cases pad16(B + r*NS) = pad16(B) + r*NS +
+// ((r*NS) >> 4), so each sub-DFT computes one padded base and the offsets of
+// its RP elements are compile-time constants.
 template <int L, int R, int RP, int NS>
 __device__ __forceinline__ void pass_scatter(const cpx (&v)[R], int j, int c, const Tile& t) {
   constexpr int S = R / RP;
+  static_assert(NS == 1 || NS * RP >= 16, "padded offsets are linear in r");
+  cpx* tb = t.s + c * t.lp;
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     const int jp = j + s * (L / R);
-    const int base = (jp / NS) * (NS * RP) + (jp & (NS - 1));
+    cpx* q = tb + pad16((jp / NS) * (NS * RP) + (jp & (NS - 1)));
 #pragma unroll
-    for (int r = 0; r < RP; ++r) t.s[t.idx(c, base + r * NS)] = v[s + r * S];
+    for (int r = 0; r < RP; ++r) q[r * NS + ((r * NS) >> 4)] = v[s + r * S];
   }
+}
+
+// Padded position of element j + r*(L/R) relative to that of element j
+// (TPT = L/R either divides 16 with j < TPT, or is a multiple of 16).
+template <int TPT>
+__host__ __device__ constexpr int nat_off(int r) {
+  return TPT >= 16 ? r * (TPT + TPT / 16) : r * TPT + ((r * TPT) >> 4);
 }
 
 template <int L, int R>
 __device__ __forceinline__ void gather_natural(cpx (&v)[R], int j, int c, const Tile& t) {
+  constexpr int TPT = L / R;
+  const cpx* q = t.s + c * t.lp + (TPT >= 16 ? pad16(j) : j);
 #pragma unroll
-  for (int r = 0; r < R; ++r) v[r] = t.s[t.idx(c, j + r * (L / R))];
+  for (int r = 0; r < R; ++r) v[r] = q[nat_off<TPT>(r)];
 }
 
 template <int L, int R>
 __device__ __forceinline__ void scatter_natural(const cpx (&v)[R], int j, int c, const Tile& t) {
+  constexpr int TPT = L / R;
+  cpx* q = t.s + c * t.lp + (TPT >= 16 ? pad16(j) : j);
 #pragma unroll
-  for (int r = 0; r < R; ++r) t.s[t.idx(c, j + r * (L / R))] = v[r];
+  for (int r = 0; r < R; ++r) q[nat_off<TPT>(r)] = v[r];
 }
 
 template <int L, int R, int NS>
@@ -579,30 +615,25 @@ struct StoreT4 {
 };
 
 // ------------------------------------------------------------------ kernel
-template <int L>
-struct RadixFor {
-  static constexpr int value = L >= 16 ? 16 : L;
+// Register budget per thread: a radix-R thread holds R complex values; with
+// 512-thread CTAs, 16 doubles-complex get 128 registers (1 CTA per SM), and
+// every halving of the state doubles the CTAs the budget allows.
+template <int R>
+struct MinBlocks {
+  // double: 128 registers at radix 16, 64 at radix 8 (and below);
+  // single: 64 at radix 16, 40 at radix 8, 64 below
+  static constexpr int value = sizeof(real) == 8 ? (R >= 16 ? 1 : 2) : (R >= 16 ? 2 : R == 8 ? 3 : 2);
 };
 
-// Register budget: 512 threads x 2 CTAs (64 registers) in single precision,
-// 512 x 1 (128 registers) in double, where each thread holds 16 complex
-// doubles.
-#if MINFFT_SINGLE
-constexpr int kMinBlocks = 2;
-#else
-constexpr int kMinBlocks = 1;
-#endif
-
-template <int L, class LoadOp, class StoreOp>
-__global__ void __launch_bounds__(512, kMinBlocks) axis_pass_kernel(const AxisParams p) {
-  constexpr int R = RadixFor<L>::value;
+template <int L, int R, class LoadOp, class StoreOp>
+__global__ void __launch_bounds__(512, MinBlocks<R>::value) axis_pass_kernel(const AxisParams p) {
+  static_assert(R <= L || L < 2, "radix at most the length");
   constexpr int TPT = L / R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   int64_t* offs = reinterpret_cast<int64_t*>(smem_raw);
   const int64_t left = p.nbatch - int64_t(blockIdx.x) * p.cpb;
   TileOffsets to{offs, offs + p.cpb, int(left < p.cpb ? left : p.cpb)};
-  Tile t{reinterpret_cast<cpx*>(smem_raw + 16 * ((2 * p.cpb * sizeof(int64_t) + 15) / 16)), p.cpb, p.colmode,
-         padded_len(L)};
+  Tile t{reinterpret_cast<cpx*>(smem_raw + 16 * ((2 * p.cpb * sizeof(int64_t) + 15) / 16)), p.lp};
 
   // offsets of the CTA's transforms, computed once per transform
   for (int c = threadIdx.x; c < p.cpb; c += blockDim.x) {
@@ -635,8 +666,8 @@ __global__ void __launch_bounds__(512, kMinBlocks) axis_pass_kernel(const AxisPa
 }
 
 // Number of bytes of dynamic shared memory the kernel needs for cpb transforms.
-inline size_t axis_pass_smem(int L, int cpb) {
-  return 16 * ((2 * cpb * sizeof(int64_t) + 15) / 16) + size_t(cpb) * padded_len(L) * sizeof(cpx);
+inline size_t axis_pass_smem(int L, int R, int cpb, int colmode) {
+  return 16 * ((2 * cpb * sizeof(int64_t) + 15) / 16) + size_t(cpb) * tile_pitch(L, R, cpb, colmode) * sizeof(cpx);
 }
 
 }  // namespace mb

@@ -7,28 +7,29 @@
 
 namespace mb {
 
-const void* axis_kernel_cplx(int log2L);
-const void* axis_kernel_r2c(int log2L);
-const void* axis_kernel_c2r(int log2L);
-const void* axis_kernel_dct2(int log2L);
-const void* axis_kernel_dct3(int log2L);
-const void* axis_kernel_t4(int log2L);
+const void* axis_kernel_cplx(int log2L, int radix16);
+const void* axis_kernel_r2c(int log2L, int radix16);
+const void* axis_kernel_c2r(int log2L, int radix16);
+const void* axis_kernel_dct2(int log2L, int radix16);
+const void* axis_kernel_dct3(int log2L, int radix16);
+const void* axis_kernel_t4(int log2L, int radix16);
 
-const void* pipe_kernel_cplx(int log2L);
-const void* pipe_kernel_r2c(int log2L);
-const void* pipe_kernel_c2r(int log2L);
-const void* pipe_kernel_dct2(int log2L);
-const void* pipe_kernel_dct3(int log2L);
-const void* pipe_kernel_t4(int log2L);
+const void* pipe_kernel_cplx(int log2L, int radix16);
+const void* pipe_kernel_r2c(int log2L, int radix16);
+const void* pipe_kernel_c2r(int log2L, int radix16);
+const void* pipe_kernel_dct2(int log2L, int radix16);
+const void* pipe_kernel_dct3(int log2L, int radix16);
+const void* pipe_kernel_t4(int log2L, int radix16);
 
-const void* pipe_kernel(int combo, int log2L) {
+const void* pipe_kernel(int combo, int log2L, int R) {
+  if (log2L < 1) return nullptr;
   switch (combo) {
-    case K_CPLX: return pipe_kernel_cplx(log2L);
-    case K_R2C: return pipe_kernel_r2c(log2L);
-    case K_C2R: return pipe_kernel_c2r(log2L);
-    case K_DCT2: return pipe_kernel_dct2(log2L);
-    case K_DCT3: return pipe_kernel_dct3(log2L);
-    case K_T4: return pipe_kernel_t4(log2L);
+    case K_CPLX: return pipe_kernel_cplx(log2L, R >= 16);
+    case K_R2C: return pipe_kernel_r2c(log2L, R >= 16);
+    case K_C2R: return pipe_kernel_c2r(log2L, R >= 16);
+    case K_DCT2: return pipe_kernel_dct2(log2L, R >= 16);
+    case K_DCT3: return pipe_kernel_dct3(log2L, R >= 16);
+    case K_T4: return pipe_kernel_t4(log2L, R >= 16);
     default: return nullptr;
   }
 }
@@ -45,14 +46,14 @@ int pipe_raw_elems(int combo, int L) {
   }
 }
 
-const void* axis_kernel(int combo, int log2L) {
+const void* axis_kernel(int combo, int log2L, int R) {
   switch (combo) {
-    case K_CPLX: return axis_kernel_cplx(log2L);
-    case K_R2C: return axis_kernel_r2c(log2L);
-    case K_C2R: return axis_kernel_c2r(log2L);
-    case K_DCT2: return axis_kernel_dct2(log2L);
-    case K_DCT3: return axis_kernel_dct3(log2L);
-    case K_T4: return axis_kernel_t4(log2L);
+    case K_CPLX: return axis_kernel_cplx(log2L, R >= 16);
+    case K_R2C: return axis_kernel_r2c(log2L, R >= 16);
+    case K_C2R: return axis_kernel_c2r(log2L, R >= 16);
+    case K_DCT2: return axis_kernel_dct2(log2L, R >= 16);
+    case K_DCT3: return axis_kernel_dct3(log2L, R >= 16);
+    case K_T4: return axis_kernel_t4(log2L, R >= 16);
     default: return nullptr;
   }
 }

@@ -16,12 +16,17 @@ enum Combo : int {
 
 constexpr int kMaxLog2L = 13;  // largest in-CTA DFT: 8192 points
 
-// Returns the kernel function for combo and log2(L), or nullptr.
-const void* axis_kernel(int combo, int log2L);
+// Returns the kernel function for combo, log2(L) and per-thread radix R (8 or
+// 16; lengths below 16 use R = L), or nullptr where the configuration does not
+// exist (more than 512 threads per transform).
+const void* axis_kernel(int combo, int log2L, int R = 16);
 
 // The persistent, software-pipelined form of the same kernels (pipe_pass.cuh),
 // for log2(L) = 1 .. 13, or nullptr.
-const void* pipe_kernel(int combo, int log2L);
+const void* pipe_kernel(int combo, int log2L, int R = 16);
+
+// Radix actually used by a kernel of length L requested with radix R.
+inline int effective_radix(int L, int R) { return L < R ? L : R; }
 
 // Raw input element size and raw elements per transform of the pipelined
 // kernel of `combo` (complex or real input, L, L+1 or 2L elements).

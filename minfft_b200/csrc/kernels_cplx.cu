@@ -1,20 +1,29 @@
-// Instantiations of the axis-pass kernel for the LoadCplx / StoreCplx combination,
-// one per in-CTA DFT length 2^0 .. 2^13.
+// Instantiations of the one-tile-per-CTA axis-pass kernel for LoadCplx / StoreCplx:
+// in-CTA DFT lengths 2^0 .. 2^13, radix 8 and 16 per thread (lengths below 16
+// use their own length as the radix; configurations above 512 threads per
+// transform do not exist).
 #include "axis_pass.cuh"
 
 namespace mb {
 
-const void* axis_kernel_cplx(int log2L) {
-  static const void* const table[] = {
-      (const void*)axis_pass_kernel<1, LoadCplx, StoreCplx>,    (const void*)axis_pass_kernel<2, LoadCplx, StoreCplx>,
-      (const void*)axis_pass_kernel<4, LoadCplx, StoreCplx>,    (const void*)axis_pass_kernel<8, LoadCplx, StoreCplx>,
-      (const void*)axis_pass_kernel<16, LoadCplx, StoreCplx>,   (const void*)axis_pass_kernel<32, LoadCplx, StoreCplx>,
-      (const void*)axis_pass_kernel<64, LoadCplx, StoreCplx>,   (const void*)axis_pass_kernel<128, LoadCplx, StoreCplx>,
-      (const void*)axis_pass_kernel<256, LoadCplx, StoreCplx>,  (const void*)axis_pass_kernel<512, LoadCplx, StoreCplx>,
-      (const void*)axis_pass_kernel<1024, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<2048, LoadCplx, StoreCplx>,
-      (const void*)axis_pass_kernel<4096, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<8192, LoadCplx, StoreCplx>,
+const void* axis_kernel_cplx(int log2L, int radix16) {
+  static const void* const table[14][2] = {
+      {(const void*)axis_pass_kernel<1, 1, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<1, 1, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<2, 2, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<2, 2, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<4, 4, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<4, 4, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<8, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<8, 8, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<16, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<16, 16, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<32, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<32, 16, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<64, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<64, 16, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<128, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<128, 16, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<256, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<256, 16, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<512, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<512, 16, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<1024, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<1024, 16, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<2048, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<2048, 16, LoadCplx, StoreCplx>},
+      {(const void*)axis_pass_kernel<4096, 8, LoadCplx, StoreCplx>, (const void*)axis_pass_kernel<4096, 16, LoadCplx, StoreCplx>},
+      {nullptr, (const void*)axis_pass_kernel<8192, 16, LoadCplx, StoreCplx>},
   };
-  return (log2L >= 0 && log2L <= 13) ? table[log2L] : nullptr;
+  return (log2L >= 0 && log2L <= 13) ? table[log2L][radix16 ? 1 : 0] : nullptr;
 }
 
 }  // namespace mb

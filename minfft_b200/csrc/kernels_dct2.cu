@@ -1,20 +1,29 @@
-// Instantiations of the axis-pass kernel for the LoadDCT2 / StoreDCT2 combination,
-// one per in-CTA DFT length 2^0 .. 2^13.
+// Instantiations of the one-tile-per-CTA axis-pass kernel for LoadDCT2 / StoreDCT2:
+// in-CTA DFT lengths 2^0 .. 2^13, radix 8 and 16 per thread (lengths below 16
+// use their own length as the radix; configurations above 512 threads per
+// transform do not exist).
 #include "axis_pass.cuh"
 
 namespace mb {
 
-const void* axis_kernel_dct2(int log2L) {
-  static const void* const table[] = {
-      (const void*)axis_pass_kernel<1, LoadDCT2, StoreDCT2>,    (const void*)axis_pass_kernel<2, LoadDCT2, StoreDCT2>,
-      (const void*)axis_pass_kernel<4, LoadDCT2, StoreDCT2>,    (const void*)axis_pass_kernel<8, LoadDCT2, StoreDCT2>,
-      (const void*)axis_pass_kernel<16, LoadDCT2, StoreDCT2>,   (const void*)axis_pass_kernel<32, LoadDCT2, StoreDCT2>,
-      (const void*)axis_pass_kernel<64, LoadDCT2, StoreDCT2>,   (const void*)axis_pass_kernel<128, LoadDCT2, StoreDCT2>,
-      (const void*)axis_pass_kernel<256, LoadDCT2, StoreDCT2>,  (const void*)axis_pass_kernel<512, LoadDCT2, StoreDCT2>,
-      (const void*)axis_pass_kernel<1024, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<2048, LoadDCT2, StoreDCT2>,
-      (const void*)axis_pass_kernel<4096, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<8192, LoadDCT2, StoreDCT2>,
+const void* axis_kernel_dct2(int log2L, int radix16) {
+  static const void* const table[14][2] = {
+      {(const void*)axis_pass_kernel<1, 1, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<1, 1, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<2, 2, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<2, 2, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<4, 4, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<4, 4, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<8, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<8, 8, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<16, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<16, 16, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<32, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<32, 16, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<64, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<64, 16, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<128, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<128, 16, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<256, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<256, 16, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<512, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<512, 16, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<1024, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<1024, 16, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<2048, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<2048, 16, LoadDCT2, StoreDCT2>},
+      {(const void*)axis_pass_kernel<4096, 8, LoadDCT2, StoreDCT2>, (const void*)axis_pass_kernel<4096, 16, LoadDCT2, StoreDCT2>},
+      {nullptr, (const void*)axis_pass_kernel<8192, 16, LoadDCT2, StoreDCT2>},
   };
-  return (log2L >= 0 && log2L <= 13) ? table[log2L] : nullptr;
+  return (log2L >= 0 && log2L <= 13) ? table[log2L][radix16 ? 1 : 0] : nullptr;
 }
 
 }  // namespace mb

@@ -1,20 +1,29 @@
-// Instantiations of the pipelined axis-pass kernel for PC2R / StoreC2R, one per
-// in-CTA DFT length 2^1 .. 2^13 (index 0 is unused).
+// Instantiations of the pipelined axis-pass kernel for PC2R / StoreC2R:
+// in-CTA DFT lengths 2^0 .. 2^13, radix 8 and 16 per thread (lengths below 16
+// use their own length as the radix; configurations above 512 threads per
+// transform do not exist).
 #include "pipe_pass.cuh"
 
 namespace mb {
 
-const void* pipe_kernel_c2r(int log2L) {
-  static const void* const table[] = {
-      nullptr,                                           (const void*)axis_pipe_kernel<2, PC2R, StoreC2R>,
-      (const void*)axis_pipe_kernel<4, PC2R, StoreC2R>,    (const void*)axis_pipe_kernel<8, PC2R, StoreC2R>,
-      (const void*)axis_pipe_kernel<16, PC2R, StoreC2R>,   (const void*)axis_pipe_kernel<32, PC2R, StoreC2R>,
-      (const void*)axis_pipe_kernel<64, PC2R, StoreC2R>,   (const void*)axis_pipe_kernel<128, PC2R, StoreC2R>,
-      (const void*)axis_pipe_kernel<256, PC2R, StoreC2R>,  (const void*)axis_pipe_kernel<512, PC2R, StoreC2R>,
-      (const void*)axis_pipe_kernel<1024, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<2048, PC2R, StoreC2R>,
-      (const void*)axis_pipe_kernel<4096, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<8192, PC2R, StoreC2R>,
+const void* pipe_kernel_c2r(int log2L, int radix16) {
+  static const void* const table[14][2] = {
+      {nullptr, nullptr},
+      {(const void*)axis_pipe_kernel<2, 2, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<2, 2, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<4, 4, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<4, 4, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<8, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<8, 8, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<16, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<16, 16, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<32, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<32, 16, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<64, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<64, 16, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<128, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<128, 16, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<256, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<256, 16, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<512, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<512, 16, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<1024, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<1024, 16, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<2048, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<2048, 16, PC2R, StoreC2R>},
+      {(const void*)axis_pipe_kernel<4096, 8, PC2R, StoreC2R>, (const void*)axis_pipe_kernel<4096, 16, PC2R, StoreC2R>},
+      {nullptr, (const void*)axis_pipe_kernel<8192, 16, PC2R, StoreC2R>},
   };
-  return (log2L >= 1 && log2L <= 13) ? table[log2L] : nullptr;
+  return (log2L >= 0 && log2L <= 13) ? table[log2L][radix16 ? 1 : 0] : nullptr;
 }
 
 }  // namespace mb

@@ -106,7 +106,7 @@ int pick_cpb(int L) {
   const int want = int(128 / sizeof(cpx));
   if (cpb < want) cpb = std::max(cpb, std::min(want, std::max(1, 512 / tpt)));
   // stay within the default 48 KiB of dynamic shared memory
-  while (cpb > 1 && mb::axis_pass_smem(L, cpb) > 48 * 1024) cpb /= 2;
+  while (cpb > 1 && mb::axis_pass_smem(L, std::min(L, 16), cpb, 1) > 48 * 1024) cpb /= 2;
   return cpb;
 }
 
@@ -168,6 +168,7 @@ MB_EXPORT int minfft_b200_dft_noalloc(const void* x, void* y, int n, int inverse
   p1.st_div = 1;
   p1.colmode = 1;
   p1.cpb = pick_cpb(r1);
+  p1.lp = mb::tile_pitch(r1, 16, p1.cpb, 1);
   p1.flags = mb::F_STAGE_ROWS | (inverse ? mb::F_CONJ_IN : 0);
 
   // pass 2: n/r2 sub-DFTs of length r2 pre-multiplied by w_n^((j mod r1) r)
@@ -195,6 +196,7 @@ MB_EXPORT int minfft_b200_dft_noalloc(const void* x, void* y, int n, int inverse
   p2.st_lobits = lobits;
   p2.colmode = 1;
   p2.cpb = pick_cpb(r2);
+  p2.lp = mb::tile_pitch(r2, 16, p2.cpb, 1);
   p2.flags = inverse ? mb::F_CONJ_OUT : 0;
 
   for (const mb::AxisParams* p : {&p1, &p2}) {
@@ -204,7 +206,8 @@ MB_EXPORT int minfft_b200_dft_noalloc(const void* x, void* y, int n, int inverse
     const unsigned block = unsigned(p->cpb * (L / R));
     const unsigned grid = unsigned((p->nbatch + p->cpb - 1) / p->cpb);
     void* args[1] = {const_cast<mb::AxisParams*>(p)};
-    if (cudaLaunchKernel(fn, dim3(grid), dim3(block), args, mb::axis_pass_smem(L, p->cpb), st) != cudaSuccess)
+    if (cudaLaunchKernel(fn, dim3(grid), dim3(block), args, mb::axis_pass_smem(L, 16, p->cpb, 1), st) !=
+        cudaSuccess)
       return fail(MINFFT_B200_ECUDA, "minfft_b200_dft_noalloc: launch failed");
   }
   return MINFFT_B200_OK;

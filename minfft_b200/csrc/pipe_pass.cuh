@@ -216,18 +216,17 @@ struct PDCT3 {
 // Shared memory of the pipelined kernel: per stage, the tile's input and
 // output offsets (2*cpb int64), then the two stages.
 __host__ __device__ inline size_t pipe_offsets_bytes(int cpb) { return 16 * ((4 * size_t(cpb) * sizeof(int64_t) + 15) / 16); }
-__host__ __device__ inline size_t pipe_stage_bytes(int L, int cpb, int e_raw, size_t raw_size) {
-  const size_t a = size_t(cpb) * padded_len(L) * sizeof(cpx);
+__host__ __device__ inline size_t pipe_stage_bytes(int L, int R, int cpb, int colmode, int e_raw, size_t raw_size) {
+  const size_t a = size_t(cpb) * tile_pitch(L, R, cpb, colmode) * sizeof(cpx);
   const size_t b = size_t(cpb) * e_raw * raw_size;
   return 16 * (((a > b ? a : b) + 15) / 16);
 }
-__host__ __device__ inline size_t pipe_smem(int L, int cpb, int e_raw, size_t raw_size) {
-  return pipe_offsets_bytes(cpb) + 2 * pipe_stage_bytes(L, cpb, e_raw, raw_size);
+__host__ __device__ inline size_t pipe_smem(int L, int R, int cpb, int colmode, int e_raw, size_t raw_size) {
+  return pipe_offsets_bytes(cpb) + 2 * pipe_stage_bytes(L, R, cpb, colmode, e_raw, raw_size);
 }
 
-template <int L, class PLoad, class StoreOp>
-__global__ void __launch_bounds__(512, kMinBlocks) axis_pipe_kernel(const AxisParams p) {
-  constexpr int R = RadixFor<L>::value;
+template <int L, int R, class PLoad, class StoreOp>
+__global__ void __launch_bounds__(512, MinBlocks<R>::value) axis_pipe_kernel(const AxisParams p) {
   constexpr int TPT = L / R;
   using Raw = typename PLoad::Raw;
   constexpr int ER = PLoad::e_raw(L);
@@ -325,7 +324,7 @@ __global__ void __launch_bounds__(512, kMinBlocks) axis_pipe_kernel(const AxisPa
     int64_t* oin = offs + s * 2 * cpb;
     TileOffsets to{oin, oin + cpb, nv};
     unsigned char* st = stages + size_t(s) * p.stage_bytes;
-    Tile tl{reinterpret_cast<cpx*>(st), cpb, p.colmode, padded_len(L)};
+    Tile tl{reinterpret_cast<cpx*>(st), p.lp};
     RawTile rt{st, cpb, p.colmode, ER};
     Ctx x;
     x.c = c;

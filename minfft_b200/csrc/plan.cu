@@ -186,11 +186,12 @@ struct TuneKey {
 struct TuneVal {
   int pipe;
   int cpb;
+  int radix;  // registers per thread: 8 or 16 complex values
 };
 
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;
-TuneVal g_default_override{-1, 0};  // minfft_b200_tune_set_default: form (-1 = heuristic) and tile
+TuneVal g_default_override{-1, 0, 16};  // minfft_b200_tune_set_default: form (-1 = heuristic), tile, radix
 thread_local const std::map<TuneKey, TuneVal>* t_force = nullptr;  // candidates under test
 
 bool tune_lookup(const TuneKey& k, TuneVal* v) {
@@ -227,6 +228,7 @@ struct Launch {
   int combo = -1;        // axis kernels: mb::Combo; line kernels: mb::LineKernel
   TuneKey key{};         // axis kernels: autotuning key
   int L = 0;             // axis kernels: in-CTA DFT length
+  int radix = 16;        // axis kernels: per-thread radix
   AxisParams ap;
   LineParams lp;
   std::string label;  // kernel and shape, for launch-level timing
@@ -389,15 +391,15 @@ struct Planner {
   }
 
   // transforms per CTA for an in-CTA DFT of length L
-  int choose_cpb(int L, bool colmode) {
-    const int R = std::min(16, L);
+  int choose_cpb(int L, bool colmode, int Rq = 16) {
+    const int R = std::min(Rq, L);
     const int tpt = L / R;
     int cpb = std::max(1, 256 / tpt);
     if (colmode) {
       const int want = int(128 / sizeof(cpx));  // 128-byte runs of adjacent columns
       if (cpb < want) cpb = std::max(cpb, std::min(want, std::max(1, 512 / tpt)));
     }
-    while (cpb > 1 && mb::axis_pass_smem(L, cpb) > (size_t)dev_max_smem) cpb /= 2;
+    while (cpb > 1 && mb::axis_pass_smem(L, R, cpb, colmode ? 1 : 0) > (size_t)dev_max_smem) cpb /= 2;
     return cpb;
   }
 
@@ -416,7 +418,7 @@ struct Planner {
     return on;
   }
 
-  int max_threads_cpb(int L) const { return std::max(1, 512 / (L / std::min(16, L))); }
+  int max_threads_cpb(int L, int R = 16) const { return std::max(1, 512 / (L / std::min(R, L))); }
 
   // largest power of two <= 16 dividing every value
   static int pow2_align(std::initializer_list<int64_t> vals) {
@@ -426,15 +428,20 @@ struct Planner {
     return a;
   }
 
-  bool pipe_fits(int combo, int L, int cpb) const {
-    return L >= 2 && mb::pipe_kernel(combo, ilog2(L)) && cpb >= 1 && cpb <= max_threads_cpb(L) &&
-           mb::pipe_smem(L, cpb, mb::pipe_raw_elems(combo, L), mb::pipe_raw_size(combo)) <= (size_t)dev_max_smem;
+  bool pipe_fits(int combo, int L, int cpb, int colmode, int R = 16) const {
+    const int Re = std::min(R, L);
+    return L >= 2 && mb::pipe_kernel(combo, ilog2(L), R) && cpb >= 1 && cpb <= max_threads_cpb(L, R) &&
+           mb::pipe_smem(L, Re, cpb, colmode, mb::pipe_raw_elems(combo, L), mb::pipe_raw_size(combo)) <=
+               (size_t)dev_max_smem;
   }
 
-  bool plain_fits(int combo, int L, int cpb, int flags) const {
-    const bool tile = (L > std::min(16, L)) || staged(combo) || (flags & mb::F_STAGE_ROWS);
-    const size_t sm = tile ? mb::axis_pass_smem(L, cpb) : size_t(16 * ((2 * cpb * sizeof(int64_t) + 15) / 16));
-    return cpb >= 1 && cpb <= max_threads_cpb(L) && sm <= (size_t)dev_max_smem;
+  bool plain_fits(int combo, int L, int cpb, int flags, int colmode, int R = 16) const {
+    const int Re = std::min(R, L);
+    const bool tile = (L > Re) || staged(combo) || (flags & mb::F_STAGE_ROWS);
+    const size_t sm =
+        tile ? mb::axis_pass_smem(L, Re, cpb, colmode) : size_t(16 * ((2 * cpb * sizeof(int64_t) + 15) / 16));
+    return mb::axis_kernel(combo, ilog2(L), R) && cpb >= 1 && cpb <= max_threads_cpb(L, R) &&
+           sm <= (size_t)dev_max_smem;
   }
 
   void add_axis_kernel(int combo, int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, bool vec_in,
@@ -443,12 +450,16 @@ struct Planner {
     const TuneKey key{combo, L, ap.colmode, ap.st_ns > 1 ? 1 : 0, (ap.flags & mb::F_STAGE_ROWS) ? 1 : 0,
                       nbatch, ap.d0, ap.in_n, ap.out_k};
     TuneVal tv;
+    int R = 16;  // per-thread radix of the one-tile-per-CTA form
     if (tune_lookup(key, &tv)) {
-      if (tv.pipe && pipe_fits(combo, L, tv.cpb)) {
-        add_pipe_kernel(combo, L, nbatch, ap, in_buf, out_buf, tv.cpb, key);
+      if (tv.pipe && pipe_fits(combo, L, tv.cpb, ap.colmode, tv.radix)) {
+        add_pipe_kernel(combo, L, nbatch, ap, in_buf, out_buf, tv.cpb, key, tv.radix);
         return;
       }
-      if (!tv.pipe && plain_fits(combo, L, tv.cpb, ap.flags)) ap.cpb = tv.cpb;
+      if (!tv.pipe && plain_fits(combo, L, tv.cpb, ap.flags, ap.colmode, tv.radix)) {
+        ap.cpb = tv.cpb;
+        R = tv.radix;
+      }
     } else {
       TuneVal ov;
       {
@@ -458,29 +469,35 @@ struct Planner {
       const bool want_pipe = ov.pipe == 1 || (ov.pipe < 0 && pipe_default());
       if (want_pipe) {
         int pc = ov.cpb > 0 ? ov.cpb : choose_pipe_cpb(combo, L, ap.colmode != 0);
-        while (pc > 1 && !pipe_fits(combo, L, pc)) pc /= 2;
-        if (pipe_fits(combo, L, pc)) {
-          add_pipe_kernel(combo, L, nbatch, ap, in_buf, out_buf, pc, key);
+        const int rr = pipe_fits(combo, L, 1, ap.colmode, ov.radix) ? ov.radix : 16;
+        while (pc > 1 && !pipe_fits(combo, L, pc, ap.colmode, rr)) pc /= 2;
+        if (pipe_fits(combo, L, pc, ap.colmode, rr)) {
+          add_pipe_kernel(combo, L, nbatch, ap, in_buf, out_buf, pc, key, rr);
           return;
         }
-      } else if (ov.pipe == 0 && ov.cpb > 0) {
-        int c = ov.cpb;
-        while (c > 1 && !plain_fits(combo, L, c, ap.flags)) c /= 2;
+      } else if (ov.pipe == 0 && (ov.cpb > 0 || ov.radix != 16)) {
+        const int rr = plain_fits(combo, L, 1, ap.flags, ap.colmode, ov.radix) ? ov.radix : 16;
+        int c = ov.cpb > 0 ? ov.cpb : choose_cpb(L, ap.colmode != 0, rr);
+        while (c > 1 && !plain_fits(combo, L, c, ap.flags, ap.colmode, rr)) c /= 2;
         ap.cpb = c;
+        R = rr;
       }
     }
     Launch ln;
     ln.key = key;
-    ln.fn = mb::axis_kernel(combo, lg);
+    ln.radix = R;
+    ln.fn = mb::axis_kernel(combo, lg, R);
     if (!ln.fn) {
       set_error(MINFFT_B200_EUNSUPPORTED, "no kernel for combo %d, L=%d", combo, L);
       ok = false;
       return;
     }
-    const int R = std::min(16, L);
-    const int tpt = L / R;
-    const bool tile = (L > R) || staged(combo) || (ap.flags & mb::F_STAGE_ROWS);
-    ln.smem = tile ? mb::axis_pass_smem(L, ap.cpb) : size_t(16 * ((2 * ap.cpb * sizeof(int64_t) + 15) / 16));
+    const int Re = std::min(R, L);
+    const int tpt = L / Re;
+    const bool tile = (L > Re) || staged(combo) || (ap.flags & mb::F_STAGE_ROWS);
+    ap.lp = mb::tile_pitch(L, Re, ap.cpb, ap.colmode);
+    ln.smem = tile ? mb::axis_pass_smem(L, Re, ap.cpb, ap.colmode)
+                   : size_t(16 * ((2 * ap.cpb * sizeof(int64_t) + 15) / 16));
     if (ln.smem > (size_t)dev_max_smem) {
       set_error(MINFFT_B200_EUNSUPPORTED, "shared memory %zu exceeds %d", ln.smem, dev_max_smem);
       ok = false;
@@ -522,8 +539,8 @@ struct Planner {
   }
 
   // transforms per tile of the pipelined kernel: two stages must fit
-  int choose_pipe_cpb(int combo, int L, bool colmode) {
-    const int R = std::min(16, L);
+  int choose_pipe_cpb(int combo, int L, bool colmode, int Rq = 16) {
+    const int R = std::min(Rq, L);
     const int tpt = L / R;
     int cpb = std::max(1, 256 / tpt);
     if (colmode) {
@@ -531,18 +548,20 @@ struct Planner {
       if (cpb < want) cpb = std::max(cpb, std::min(want, std::max(1, 512 / tpt)));
     }
     const int er = mb::pipe_raw_elems(combo, L);
-    while (cpb > 1 && mb::pipe_smem(L, cpb, er, mb::pipe_raw_size(combo)) > (size_t)dev_max_smem) cpb /= 2;
+    while (cpb > 1 && mb::pipe_smem(L, R, cpb, colmode ? 1 : 0, er, mb::pipe_raw_size(combo)) > (size_t)dev_max_smem)
+      cpb /= 2;
     return cpb;
   }
 
   void add_pipe_kernel(int combo, int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, int cpb,
-                       const TuneKey& key) {
+                       const TuneKey& key, int Rq = 16) {
     const int lg = ilog2(L);
     Launch ln;
     ln.key = key;
-    ln.fn = mb::pipe_kernel(combo, lg);
+    ln.radix = Rq;
+    ln.fn = mb::pipe_kernel(combo, lg, Rq);
     ln.pipe = true;
-    const int R = std::min(16, L);
+    const int R = std::min(Rq, L);
     const int tpt = L / R;
     const int esz = mb::pipe_raw_size(combo), er = mb::pipe_raw_elems(combo, L);
     ap.cpb = cpb;
@@ -557,8 +576,9 @@ struct Planner {
       const int64_t run = int64_t(er % 2 == 1 ? er - 1 : er) * esz;
       ln.ch_static = pow2_align({run, int64_t(er) * esz, ap.is1 * esz, ap.is2 * esz});
     }
-    ap.stage_bytes = (int)mb::pipe_stage_bytes(L, ap.cpb, er, esz);
-    ln.smem = mb::pipe_smem(L, ap.cpb, er, esz);
+    ap.lp = mb::tile_pitch(L, R, ap.cpb, ap.colmode);
+    ap.stage_bytes = (int)mb::pipe_stage_bytes(L, R, ap.cpb, ap.colmode, er, esz);
+    ln.smem = mb::pipe_smem(L, R, ap.cpb, ap.colmode, er, esz);
     if (ln.smem > (size_t)dev_max_smem) {
       set_error(MINFFT_B200_EUNSUPPORTED, "shared memory %zu exceeds %d", ln.smem, dev_max_smem);
       ok = false;
@@ -1511,6 +1531,8 @@ MB_EXPORT int minfft_b200_plan_selfcheck(int op, int d, const int* Ns, int howma
            (long long)((e.out_max + 1) * oe), ln.out_buf, cap[ln.out_buf]);
     if (ln.block < 1 || ln.block > 1024 || ln.grid < 1) fail("launch %zu: bad shape %u x %u", i, ln.grid, ln.block);
     if (!ln.is_line && ln.block > 512) fail("launch %zu: block %u above launch bounds", i, ln.block);
+    if (!ln.is_line && ln.block != unsigned(ln.ap.cpb * (ln.L / std::min(ln.radix, std::max(ln.L, 1)))))
+      fail("launch %zu: block %u is not cpb x L/R", i, ln.block);
     if (ln.smem > size_t(di.max_smem)) fail("launch %zu: %zu bytes of shared memory", i, ln.smem);
     const bool alias_io = (ln.in_buf == ln.out_buf) || (alias && ((ln.in_buf == BUF_X && ln.out_buf == BUF_Y) ||
                                                                  (ln.in_buf == BUF_Y && ln.out_buf == BUF_X)));
@@ -1533,7 +1555,8 @@ MB_EXPORT int minfft_b200_plan_selfcheck(int op, int d, const int* Ns, int howma
       if (ln.ch_static < esz && ln.ch_static < 16 && esz <= 16 && ln.ch_static % 4 != 0)
         fail("launch %zu: copy chunk %d", i, ln.ch_static);
       if (size_t(ap.stage_bytes) < size_t(ap.cpb) * mb::pipe_raw_elems(ln.combo, ln.L) * esz ||
-          size_t(ap.stage_bytes) < size_t(ap.cpb) * mb::padded_len(ln.L) * sizeof(cpx))
+          size_t(ap.stage_bytes) <
+              size_t(ap.cpb) * mb::tile_pitch(ln.L, std::min(ln.radix, ln.L), ap.cpb, ap.colmode) * sizeof(cpx))
         fail("launch %zu: stage of %d bytes too small", i, ap.stage_bytes);
     }
   }
@@ -1604,13 +1627,16 @@ MB_EXPORT int minfft_b200_autotune(minfft_aux* a, int op, int howmany, int reps)
     if (best.count(key)) continue;
     Planner probe{a, nullptr, di.max_smem, di.sms};
     float best_ms = 1e30f;
-    TuneVal best_v{0, 0};
-    for (int pipe = 0; pipe <= 1; ++pipe) {
-      for (int cpb = 1; cpb <= probe.max_threads_cpb(key.L); cpb *= 2) {
-        const bool fits = pipe ? probe.pipe_fits(key.combo, key.L, cpb)
-                               : probe.plain_fits(key.combo, key.L, cpb, key.staged ? mb::F_STAGE_ROWS : 0);
+    TuneVal best_v{0, 0, 16};
+    for (int cand = 0; cand < 4; ++cand) {
+      const int pipe = cand & 1, radix = (cand & 2) ? 8 : 16;
+      if (radix == 8 && key.L <= 8) continue;
+      for (int cpb = 1; cpb <= probe.max_threads_cpb(key.L, radix); cpb *= 2) {
+        const bool fits = pipe ? probe.pipe_fits(key.combo, key.L, cpb, key.colmode, radix)
+                               : probe.plain_fits(key.combo, key.L, cpb, key.staged ? mb::F_STAGE_ROWS : 0,
+                                                  key.colmode, radix);
         if (!fits) continue;
-        force[key] = TuneVal{pipe, cpb};
+        force[key] = TuneVal{pipe, cpb, radix};
         Program P;
         if (!build_program(a, op, howmany, false, &P)) continue;
         bool bufs_ok = true;
@@ -1625,7 +1651,7 @@ MB_EXPORT int minfft_b200_autotune(minfft_aux* a, int op, int howmany, int reps)
           const float ms = time_launch(a, ln, bufs, reps);
           if (ms > 0 && ms < best_ms) {
             best_ms = ms;
-            best_v = TuneVal{pipe, cpb};
+            best_v = TuneVal{pipe, cpb, radix};
           }
           break;
         }
@@ -1656,13 +1682,13 @@ MB_EXPORT int minfft_b200_tune_save(const char* path) {
     return MINFFT_B200_EINVAL;
   }
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  fprintf(f, "# minfft_b200 tuning table (%s): combo L colmode hbm staged nbatch d0 in_n out_k pipe cpb\n",
+  fprintf(f, "# minfft_b200 tuning table (%s): combo L colmode hbm staged nbatch d0 in_n out_k pipe cpb radix\n",
           sizeof(real) == 8 ? "double" : "single");
   for (auto& kv : g_tune) {
     const TuneKey& k = kv.first;
-    fprintf(f, "%d %d %d %d %d %lld %lld %lld %lld %d %d\n", k.combo, k.L, k.colmode, k.hbm, k.staged,
+    fprintf(f, "%d %d %d %d %d %lld %lld %lld %lld %d %d %d\n", k.combo, k.L, k.colmode, k.hbm, k.staged,
             (long long)k.nbatch, (long long)k.d0, (long long)k.in_n, (long long)k.out_k, kv.second.pipe,
-            kv.second.cpb);
+            kv.second.cpb, kv.second.radix);
   }
   fclose(f);
   return MINFFT_B200_OK;
@@ -1682,8 +1708,9 @@ MB_EXPORT int minfft_b200_tune_load(const char* path) {
     TuneKey k{};
     TuneVal v{};
     long long nb, d0, in_n, out_k;
-    if (sscanf(line, "%d %d %d %d %d %lld %lld %lld %lld %d %d", &k.combo, &k.L, &k.colmode, &k.hbm, &k.staged, &nb,
-               &d0, &in_n, &out_k, &v.pipe, &v.cpb) == 11) {
+    if (sscanf(line, "%d %d %d %d %d %lld %lld %lld %lld %d %d %d", &k.combo, &k.L, &k.colmode, &k.hbm, &k.staged,
+               &nb, &d0, &in_n, &out_k, &v.pipe, &v.cpb, &v.radix) == 12 &&
+        (v.radix == 8 || v.radix == 16)) {
       k.nbatch = nb;
       k.d0 = d0;
       k.in_n = in_n;
@@ -1708,10 +1735,11 @@ MB_EXPORT int minfft_b200_tune_size(void) {
 
 // Launch configuration used where the tuning table has no entry: pipe = 1
 // persistent pipelined kernels, 0 one tile per CTA, -1 the planner's choice;
-// cpb > 0 sets transforms per CTA (reduced until it fits), 0 the heuristic.
-// Plans built afterwards use it.
-MB_EXPORT int minfft_b200_tune_set_default(int pipe, int cpb) {
+// cpb > 0 sets transforms per CTA (reduced until it fits), 0 the heuristic;
+// radix 8 or 16 registers per thread (16 where 8 does not exist).  Plans
+// built afterwards use it.
+MB_EXPORT int minfft_b200_tune_set_default(int pipe, int cpb, int radix) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_default_override = TuneVal{pipe < 0 ? -1 : (pipe ? 1 : 0), cpb < 0 ? 0 : cpb};
+  g_default_override = TuneVal{pipe < 0 ? -1 : (pipe ? 1 : 0), cpb < 0 ? 0 : cpb, radix == 8 ? 8 : 16};
   return MINFFT_B200_OK;
 }

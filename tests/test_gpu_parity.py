@@ -332,21 +332,23 @@ def test_autotuned_plans_stay_correct(single, tmp_path):
 
 @pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
 @pytest.mark.parametrize("pipe", [0, 1], ids=["tile", "pipelined"])
-def test_every_forced_configuration_is_correct(single, pipe):
-    """Both kernel forms at every tile size (transforms per CTA), forced as the
-    default configuration, on row and column passes of every transform kind."""
+@pytest.mark.parametrize("radix", [8, 16])
+def test_every_forced_configuration_is_correct(single, pipe, radix):
+    """Both kernel forms, both per-thread radices, at every tile size
+    (transforms per CTA), forced as the default configuration, on row and
+    column passes of every transform kind."""
     eng = minfft_b200.engine(single)
     rng = np.random.default_rng(43)
     saved = eng.tune_size()
     try:
         eng.tune_clear()
         for cpb in (1, 2, 4, 8, 16, 64):
-            eng.tune_set_default(pipe, cpb)
+            eng.tune_set_default(pipe, cpb, radix)
             for dims in [(64, 512), (8, 2048), (1 << 14,)]:
                 for op in OPS:
                     x = make_input(op, dims, rng, single)
                     err = rel_l2(gpu_apply(op, x, dims, single), expected(op, x, dims))
                     assert err <= tolerance(single, dims), (op, dims, cpb, err)
     finally:
-        eng.tune_set_default(-1, 0)
+        eng.tune_set_default(-1, 0, 16)
     assert saved >= 0

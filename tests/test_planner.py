@@ -64,12 +64,13 @@ def test_selfcheck_rejects_bad_arguments():
 
 @pytest.mark.parametrize("single", [False, True], ids=["double", "single"])
 @pytest.mark.parametrize("pipe", [0, 1], ids=["tile", "pipelined"])
-def test_every_launch_configuration_is_in_bounds(single, pipe):
-    """Every kernel form and tile size the autotuner may pick, on every shape."""
+@pytest.mark.parametrize("radix", [8, 16])
+def test_every_launch_configuration_is_in_bounds(single, pipe, radix):
+    """Every kernel form, radix and tile size the autotuner may pick, on every shape."""
     eng = minfft_b200.engine(single)
     try:
         for cpb in (1, 2, 4, 8, 16, 32, 64, 128, 256, 512):
-            eng.tune_set_default(pipe, cpb)
+            eng.tune_set_default(pipe, cpb, radix)
             for dims in SHAPES + HUGE[:3]:
                 for op in OPS:
                     for alias in (False, True):
