@@ -155,6 +155,15 @@ class Workload2D:
             yield p["eng"], p["pr"], ("realdft", "invrealdft")
             yield p["eng"], p["pt"], ("dct2", "dct3")
 
+    def rebuild(self, eng, plan):
+        """Replace `plan` by a fresh one (launch lists follow the current tuning table)."""
+        for p in self.precs:
+            for key in ("pr", "pt"):
+                if p[key] is plan:
+                    fam = plan.family
+                    plan.free()
+                    p[key] = eng.plan(fam, self.dims)
+
     def step(self, k: int):
         s = k % self.nsets
         for p in self.precs:
@@ -241,6 +250,10 @@ class WorkloadBatch4096:
 
     def howmany_for(self, op):
         return self.howmany
+
+    def rebuild(self, eng, plan):
+        self.plan.free()
+        self.plan = eng.plan("dft", (self.n,))
 
     def step(self, k):
         x = self.xs[k % self.nsets]
@@ -374,12 +387,22 @@ def run_engine(args):
 
     W = WORKLOADS[args.workload](torch, dev)
     tuned = 0
-    if not args.no_tune:
-        # project autotuner: pick kernel form and tile size per launch (setup, untimed)
+    if args.tune_file and all(os.path.exists(f"{args.tune_file}.{'f32' if s else 'f64'}") for s in (False, True)):
+        # reuse a saved tuning table (e.g. for deterministic profiling runs)
+        for eng, plan, ops in W.plans():
+            eng.tune_load(f"{args.tune_file}.{'f32' if eng.single else 'f64'}")
+            tuned = max(tuned, eng.tune_size())
+        for eng, plan, ops in W.plans():
+            W.rebuild(eng, plan)
+    elif not args.no_tune:
+        # project autotuner: pick kernel form, radix and tile size per launch (setup, untimed)
         for eng, plan, ops in W.plans():
             for op in ops:
                 eng.autotune(plan.aux, op, getattr(W, "howmany_for", lambda o: 1)(op), 5)
             tuned = max(tuned, eng.tune_size())
+        if args.tune_file:
+            for eng, plan, ops in W.plans():
+                eng.tune_save(f"{args.tune_file}.{'f32' if eng.single else 'f64'}")
     launches_per_step = W.launches_per_step()
 
     # warm-up
@@ -505,6 +528,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (heuristic launch configurations)")
+    ap.add_argument("--tune-file", default="", help="tuning table prefix: loaded if present, else saved after tuning")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -228,11 +228,20 @@ struct LoadCplx {
   static constexpr bool kStaged = false;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+    constexpr int TPT = L / R;
     const cpx* in = static_cast<const cpx*>(p.in) + x.oin;
+    if (!x.active) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int64_t n = x.j + r * (L / R);
-      v[r] = x.active ? __ldcs(in + n * p.in_n) : czero();
+      for (int r = 0; r < R; ++r) v[r] = czero();
+    } else if (p.in_n == 1) {  // contiguous: compile-time offsets
+      const cpx* q = in + x.j;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = __ldcs(q + r * TPT);
+    } else {
+      const cpx* q = in + x.j * p.in_n;
+      const int64_t st = int64_t(TPT) * p.in_n;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = __ldcs(q + r * st);
     }
     if (p.flags & F_CONJ_IN) {
 #pragma unroll
@@ -260,17 +269,19 @@ struct LoadR2C {
   static constexpr bool kStaged = false;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+    constexpr int TPT = L / R;
     const real* in = static_cast<const real*>(p.in) + x.oin;
-    const bool vec = (p.flags & F_VEC) != 0;
+    if (!x.active) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int n = x.j + r * (L / R);
-      if (!x.active)
-        v[r] = czero();
-      else if (vec)
-        v[r] = __ldcs(reinterpret_cast<const cpx*>(in) + n);
-      else
-        v[r] = cmk(in[2 * n], in[2 * n + 1]);
+      for (int r = 0; r < R; ++r) v[r] = czero();
+    } else if (p.flags & F_VEC) {
+      const cpx* q = reinterpret_cast<const cpx*>(in) + x.j;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = __ldcs(q + r * TPT);
+    } else {
+      const real* q = in + 2 * x.j;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = cmk(q[2 * r * TPT], q[2 * r * TPT + 1]);
     }
   }
 };
@@ -285,17 +296,28 @@ struct LoadDCT2 {
     const real* in = static_cast<const real*>(p.in) + x.oin;
     const real sg = (p.flags & F_DST) ? real(-1) : real(1);
     constexpr int N = 2 * L;
+    constexpr int TPT = L / R;
+    if (!x.active) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int m = x.j + r * (L / R);
-      if (!x.active) {
-        v[r] = czero();
-        continue;
+      for (int r = 0; r < R; ++r) v[r] = czero();
+      return;
+    }
+    if constexpr (L >= 2) {
+      // element m = j + r*TPT lies in the first half (m < L/2) exactly when r < R/2:
+      // pair (x[4m], x[4m+2]) there, (x[2N-1-4m], x[2N-3-4m]) (times sg) after
+      const int64_t s = p.in_n;
+      const real* lo = in + int64_t(4 * x.j) * s;
+      const real* hi = in + int64_t(2 * N - 1 - 4 * x.j) * s;
+      const int64_t st = int64_t(4 * TPT) * s;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (r < R / 2)
+          v[r] = cmk(lo[r * st], lo[r * st + 2 * s]);
+        else
+          v[r] = cmk(sg * hi[-r * st], sg * hi[-r * st - 2 * s]);
       }
-      const int i0 = 2 * m, i1 = 2 * m + 1;
-      const real a = i0 < L ? in[int64_t(2 * i0) * p.in_n] : sg * in[int64_t(2 * N - 1 - 2 * i0) * p.in_n];
-      const real b = i1 < L ? in[int64_t(2 * i1) * p.in_n] : sg * in[int64_t(2 * N - 1 - 2 * i1) * p.in_n];
-      v[r] = cmk(a, b);
+    } else {
+      v[0] = cmk(in[0], sg * in[p.in_n]);  // L = 1: u = (x0, +-x1)
     }
   }
 };
@@ -310,20 +332,26 @@ struct LoadT4 {
     const real* in = static_cast<const real*>(p.in) + x.oin;
     const bool dst = (p.flags & F_DST) != 0;
     constexpr int N = 2 * L;
+    constexpr int TPT = L / R;
+    if (!x.active) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = czero();
+      return;
+    }
+    const int64_t s = p.in_n;
+    const real* lo = in + int64_t(2 * x.j) * s;
+    const real* hi = in + int64_t(N - 1 - 2 * x.j) * s;
+    const int64_t st = int64_t(2 * TPT) * s;
+    const cpx* e = p.t1 + x.j;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int n = x.j + r * (L / R);
-      if (!x.active) {
-        v[r] = czero();
-        continue;
-      }
-      const real a = in[int64_t(2 * n) * p.in_n];
-      const real b = in[int64_t(N - 1 - 2 * n) * p.in_n];
-      const cpx e = ldg(p.t1 + n);
+      const real a = lo[r * st];
+      const real b = hi[-r * st];
+      const cpx w = ldg(e + r * TPT);
       if (!dst) {
-        v[r] = cmul(e, cmk(a, b));
+        v[r] = cmul(w, cmk(a, b));
       } else {
-        const cpx q = cmul(e, cmk(a, -b));
+        const cpx q = cmul(w, cmk(a, -b));
         v[r] = cmk(-q.x, -q.y);
       }
     }
@@ -353,6 +381,37 @@ __device__ __forceinline__ void unpack_pair(cpx za, cpx zb, cpx f, cpx& xa, cpx&
   xb = cconj(csub(u, vv));
 }
 
+// Visits the spectrum pairs (k, L-k), k = 0 .. L/2, owned by thread j of a
+// transform: k = j + i*TPT for i = 0 .. R/2 (only j = 0 reaches k = L/2).
+// zf(k) reads a spectrum value -- for k = 0 also zf(L), which readers of an
+// L-element tile must fold back into range; body(k, z_k, z_{L-k}) consumes
+// the pair.
+template <int L, int R, class Zf, class Body>
+__device__ __forceinline__ void pair_loop(const Ctx& x, const Zf& zf, const Body& body) {
+  constexpr int TPT = L / R;
+#pragma unroll
+  for (int i = 0; i <= R / 2; ++i) {
+    const int k = x.j + i * TPT;
+    if (i == R / 2 && x.j != 0) break;
+    body(k, zf(k), zf(L - k));
+  }
+}
+
+// Packs the pair (z_k, z_{L-k}) into the conjugated inverse-DFT inputs t_k,
+// t_{L-k} of the tile (k = 0 and k = L/2 are the self-paired ends).
+__device__ __forceinline__ void pack_into(const Tile& t, int c, int k, int L, cpx z0, cpx z1, const cpx* f) {
+  if (k == 0) {
+    t.s[t.idx(c, 0)] = cmk(z0.x + z1.x, -(z0.x - z1.x));
+  } else if (2 * k == L) {
+    t.s[t.idx(c, k)] = cmk(2 * z0.x, 2 * z0.y);
+  } else {
+    cpx ta, tb;
+    pack_pair(z0, z1, ldg(f + k), ta, tb);
+    t.s[t.idx(c, k)] = cconj(ta);
+    t.s[t.idx(c, L - k)] = cconj(tb);
+  }
+}
+
 // Inverse real DFT input: spectrum X_k, k = 0..L, packed into L complex
 // values, staged in shared memory.  Stored conjugated: the inverse DFT is
 // computed as conj(DFT(conj(t))).  t2 = w_N^k, k < L/2.
@@ -361,23 +420,8 @@ struct LoadC2R {
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
     const cpx* in = static_cast<const cpx*>(p.in) + x.oin;
-    for (int k = x.j; k <= L / 2; k += L / R) {
-      cpx z0 = czero(), z1 = czero();
-      if (x.active) {
-        z0 = in[int64_t(k) * p.in_n];
-        z1 = in[int64_t(L - k) * p.in_n];
-      }
-      if (k == 0) {
-        t.s[t.idx(x.c, 0)] = cmk(z0.x + z1.x, -(z0.x - z1.x));
-      } else if (2 * k == L) {
-        t.s[t.idx(x.c, k)] = cmk(2 * z0.x, 2 * z0.y);
-      } else {
-        cpx ta, tb;
-        pack_pair(z0, z1, ldg(p.t2 + k), ta, tb);
-        t.s[t.idx(x.c, k)] = cconj(ta);
-        t.s[t.idx(x.c, L - k)] = cconj(tb);
-      }
-    }
+    pair_loop<L, R>(x, [&](int k) { return x.active ? in[int64_t(k) * p.in_n] : czero(); },
+                    [&](int k, cpx z0, cpx z1) { pack_into(t, x.c, k, L, z0, z1, p.t2); });
     __syncthreads();
     gather_natural<L, R>(v, x.j, x.c, t);
   }
@@ -408,23 +452,8 @@ struct LoadDCT3 {
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
     const real* in = static_cast<const real*>(p.in) + x.oin;
     const bool dst = (p.flags & F_DST) != 0;
-    for (int k = x.j; k <= L / 2; k += L / R) {
-      cpx z0 = czero(), z1 = czero();
-      if (x.active) {
-        z0 = zval(in, p.in_n, k, L, dst, p.t1);
-        z1 = zval(in, p.in_n, L - k, L, dst, p.t1);
-      }
-      if (k == 0) {
-        t.s[t.idx(x.c, 0)] = cmk(z0.x + z1.x, -(z0.x - z1.x));
-      } else if (2 * k == L) {
-        t.s[t.idx(x.c, k)] = cmk(2 * z0.x, 2 * z0.y);
-      } else {
-        cpx ta, tb;
-        pack_pair(z0, z1, ldg(p.t2 + k), ta, tb);
-        t.s[t.idx(x.c, k)] = cconj(ta);
-        t.s[t.idx(x.c, L - k)] = cconj(tb);
-      }
-    }
+    pair_loop<L, R>(x, [&](int k) { return x.active ? zval(in, p.in_n, k, L, dst, p.t1) : czero(); },
+                    [&](int k, cpx z0, cpx z1) { pack_into(t, x.c, k, L, z0, z1, p.t2); });
     __syncthreads();
     gather_natural<L, R>(v, x.j, x.c, t);
   }
@@ -450,12 +479,20 @@ struct StoreCplx {
     const bool cj = (p.flags & F_CONJ_OUT) != 0;
     if (!(p.flags & F_STAGE_ROWS)) {
       if (!x.active) return;
+      constexpr int TPT = L / R;
+      if (cj) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int64_t k = x.j + r * (L / R);
-        cpx o = v[r];
-        if (cj) o.y = -o.y;
-        out[x.oout + k * p.out_k] = o;
+        for (int r = 0; r < R; ++r) v[r].y = -v[r].y;
+      }
+      if (p.out_k == 1) {
+        cpx* q = out + x.oout + x.j;
+#pragma unroll
+        for (int r = 0; r < R; ++r) q[r * TPT] = v[r];
+      } else {
+        cpx* q = out + x.oout + x.j * p.out_k;
+        const int64_t st = int64_t(TPT) * p.out_k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) q[r * st] = v[r];
       }
       return;
     }
@@ -484,8 +521,7 @@ struct StoreR2C {
     __syncthreads();
     if (!x.active) return;
     cpx* out = static_cast<cpx*>(p.out) + x.oout;
-    for (int k = x.j; k <= L / 2; k += L / R) {
-      const cpx za = t.s[t.idx(x.c, k)];
+    pair_loop<L, R>(x, [&](int k) { return t.s[t.idx(x.c, k & (L - 1))]; }, [&](int k, cpx za, cpx zb) {
       if (k == 0) {
         out[0] = cmk(za.x + za.y, real(0));
         out[int64_t(L) * p.out_k] = cmk(za.x - za.y, real(0));
@@ -493,11 +529,11 @@ struct StoreR2C {
         out[int64_t(k) * p.out_k] = cconj(za);
       } else {
         cpx xa, xb;
-        unpack_pair(za, t.s[t.idx(x.c, L - k)], ldg(p.t1 + k), xa, xb);
+        unpack_pair(za, zb, ldg(p.t1 + k), xa, xb);
         out[int64_t(k) * p.out_k] = xa;
         out[int64_t(L - k) * p.out_k] = xb;
       }
-    }
+    });
   }
 };
 
@@ -526,8 +562,7 @@ struct StoreDCT2 {
     const bool dst = (p.flags & F_DST) != 0;
     constexpr int N = 2 * L;
     const real r2 = real(1.414213562373095048801688724209698079);
-    for (int k = x.j; k <= L / 2; k += L / R) {
-      const cpx za = t.s[t.idx(x.c, k)];
+    pair_loop<L, R>(x, [&](int k) { return t.s[t.idx(x.c, k & (L - 1))]; }, [&](int k, cpx za, cpx zb) {
       if (k == 0) {
         const real v0 = za.x + za.y, vl = za.x - za.y;
         out[int64_t(dst ? N - 1 : 0) * p.out_k] = 2 * v0;
@@ -536,11 +571,11 @@ struct StoreDCT2 {
         emit(out, p.out_k, k, N, dst, cconj(za), ldg(p.t1 + k));
       } else {
         cpx xa, xb;
-        unpack_pair(za, t.s[t.idx(x.c, L - k)], ldg(p.t2 + k), xa, xb);
+        unpack_pair(za, zb, ldg(p.t2 + k), xa, xb);
         emit(out, p.out_k, k, N, dst, xa, ldg(p.t1 + k));
         emit(out, p.out_k, L - k, N, dst, xb, ldg(p.t1 + L - k));
       }
-    }
+    });
   }
 };
 
@@ -551,17 +586,18 @@ struct StoreC2R {
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, const TileOffsets&,
                                              cpx (&v)[R]) {
     if (!x.active) return;
+    constexpr int TPT = L / R;
     real* out = static_cast<real*>(p.out) + x.oout;
-    const bool vec = (p.flags & F_VEC) != 0;
+    if (p.flags & F_VEC) {
+      cpx* q = reinterpret_cast<cpx*>(out) + x.j;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int m = x.j + r * (L / R);
-      const cpx w = cconj(v[r]);
-      if (vec) {
-        reinterpret_cast<cpx*>(out)[m] = w;
-      } else {
-        out[2 * m] = w.x;
-        out[2 * m + 1] = w.y;
+      for (int r = 0; r < R; ++r) q[r * TPT] = cconj(v[r]);
+    } else {
+      real* q = out + 2 * x.j;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        q[2 * r * TPT] = v[r].x;
+        q[2 * r * TPT + 1] = -v[r].y;
       }
     }
   }
@@ -578,15 +614,30 @@ struct StoreDCT3 {
     real* out = static_cast<real*>(p.out) + x.oout;
     const bool dst = (p.flags & F_DST) != 0;
     constexpr int N = 2 * L;
+    constexpr int TPT = L / R;
+    if constexpr (L >= 2) {
+      // reals t_2m, t_2m+1 (m = j + r*TPT) go to y[4m], y[4m+2] while r < R/2,
+      // else to y[2N-1-4m], y[2N-3-4m] (negated for DST-3)
+      const real sg = dst ? real(-1) : real(1);
+      const int64_t s = p.out_k;
+      real* lo = out + int64_t(4 * x.j) * s;
+      real* hi = out + int64_t(2 * N - 1 - 4 * x.j) * s;
+      const int64_t st = int64_t(4 * TPT) * s;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int m = x.j + r * (L / R);
-      const cpx w = cconj(v[r]);
-      const int i0 = 2 * m, i1 = 2 * m + 1;
-      const real a = (dst && i0 >= L) ? -w.x : w.x;
-      const real b = (dst && i1 >= L) ? -w.y : w.y;
-      out[int64_t(i0 < L ? 2 * i0 : 2 * N - 1 - 2 * i0) * p.out_k] = a;
-      out[int64_t(i1 < L ? 2 * i1 : 2 * N - 1 - 2 * i1) * p.out_k] = b;
+      for (int r = 0; r < R; ++r) {
+        const cpx w = cconj(v[r]);
+        if (r < R / 2) {
+          lo[r * st] = w.x;
+          lo[r * st + 2 * s] = w.y;
+        } else {
+          hi[-r * st] = sg * w.x;
+          hi[-r * st - 2 * s] = sg * w.y;
+        }
+      }
+    } else {  // L = 1: y0 = t0, y1 = +-t1
+      const cpx w = cconj(v[0]);
+      out[0] = w.x;
+      out[p.out_k] = dst ? -w.y : w.y;
     }
   }
 };
@@ -602,14 +653,20 @@ struct StoreT4 {
     real* out = static_cast<real*>(p.out) + x.oout;
     const bool dst = (p.flags & F_DST) != 0;
     constexpr int N = 2 * L;
+    constexpr int TPT = L / R;
+    const int64_t s = p.out_k;
+    real* lo = out + int64_t(2 * x.j) * s;
+    real* hi = out + int64_t(N - 1 - 2 * x.j) * s;
+    const int64_t st = int64_t(2 * TPT) * s;
+    const cpx* glo = p.t2 + 2 * x.j;
+    const cpx* ghi = p.t2 + (N - 1 - 2 * x.j);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int m = x.j + r * (L / R);
       const cpx T = v[r];
-      const cpx a = cmul(ldg(p.t2 + 2 * m), T);
-      const cpx b = cmul(ldg(p.t2 + (N - 1 - 2 * m)), cconj(T));
-      out[int64_t(2 * m) * p.out_k] = 2 * (dst ? a.y : a.x);
-      out[int64_t(N - 1 - 2 * m) * p.out_k] = 2 * (dst ? b.y : b.x);
+      const cpx a = cmul(ldg(glo + 2 * r * TPT), T);
+      const cpx b = cmul(ldg(ghi - 2 * r * TPT), cconj(T));
+      lo[r * st] = 2 * (dst ? a.y : a.x);
+      hi[-r * st] = 2 * (dst ? b.y : b.x);
     }
   }
 };
