@@ -104,6 +104,33 @@ int minfft_b200_profile_entry(minfft_aux *a, int i, const char **label, long lon
  * with nothing launched. */
 int minfft_b200_dft_noalloc(const void *x, void *y, int n, int inverse, void *stream);
 
+/* ----------------------------------------------------------- mixed batch */
+/* Thousands of independent 1-D transforms of any kind and power-of-two
+ * length in one persistent kernel launched from a CUDA graph.  Each job names
+ * a transform code (MINFFT_B200_*), its length n (1 .. 65536 for complex
+ * transforms, 1 .. 131072 for the real ones) and device input and output
+ * arrays (complex data aligned to its size).  Jobs are grouped by kind and
+ * length into work items (up to 512*16/L short transforms per item; one item
+ * per transform longer than 8192 complex points, which its CTA computes in
+ * two passes through a private scratch slice) and handed out through an
+ * atomic queue, largest items first.  The plan owns the root tables, the
+ * queue and the scratch; execute only launches the captured graph on
+ * `stream`.  Outputs of different jobs must not overlap their inputs. */
+typedef struct {
+    int op;
+    int n;
+    const void *in;
+    void *out;
+} minfft_b200_job;
+typedef struct minfft_b200_mixed minfft_b200_mixed;
+minfft_b200_mixed *minfft_b200_mixed_plan(int count, const minfft_b200_job *jobs);
+int minfft_b200_mixed_execute(minfft_b200_mixed *m, void *stream);
+/* Time tile shapes (jobs per short work item) and persistent grid sizes
+ * (CTAs per SM) on the plan's own data and keep the fastest. */
+int minfft_b200_mixed_autotune(minfft_b200_mixed *m, int reps);
+int minfft_b200_mixed_items(const minfft_b200_mixed *m);
+void minfft_b200_mixed_free(minfft_b200_mixed *m);
+
 /* ------------------------------------------------------------- autotuner */
 /* Time the candidate launch configurations (kernel form: one tile per CTA
  * or persistent CTAs with double-buffered asynchronous copies; per-thread

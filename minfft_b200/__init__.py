@@ -35,6 +35,12 @@ class MinfftError(RuntimeError):
         self.code = code
 
 
+class MixedJob(ctypes.Structure):
+    """One job of a mixed batch (minfft_b200_job): transform code, length, device pointers."""
+
+    _fields_ = [("op", ctypes.c_int), ("n", ctypes.c_int), ("inp", ctypes.c_void_p), ("out", ctypes.c_void_p)]
+
+
 class Engine(MinfftLibrary):
     """One loaded engine library (one precision) with its extension API bound."""
 
@@ -84,6 +90,16 @@ class Engine(MinfftLibrary):
         L.minfft_b200_tune_size.restype = i32
         L.minfft_b200_tune_set_default.argtypes = [i32, i32, i32]
         L.minfft_b200_tune_set_default.restype = i32
+        L.minfft_b200_mixed_plan.argtypes = [i32, ctypes.POINTER(MixedJob)]
+        L.minfft_b200_mixed_plan.restype = vp
+        L.minfft_b200_mixed_execute.argtypes = [vp, vp]
+        L.minfft_b200_mixed_execute.restype = i32
+        L.minfft_b200_mixed_autotune.argtypes = [vp, i32]
+        L.minfft_b200_mixed_autotune.restype = i32
+        L.minfft_b200_mixed_items.argtypes = [vp]
+        L.minfft_b200_mixed_items.restype = i32
+        L.minfft_b200_mixed_free.argtypes = [vp]
+        L.minfft_b200_mixed_free.restype = None
 
     # --------------------------------------------------------- errors
     def last_error(self) -> int:
@@ -168,6 +184,31 @@ class Engine(MinfftLibrary):
                 self.check()
             out.append((lab.value.decode(), int(cnt.value), float(ms.value), float(by.value)))
         return out
+
+    # ----------------------------------------------------- mixed batches
+    def mixed_plan(self, jobs) -> int:
+        """Plan a mixed batch from (op, n, in_ptr, out_ptr) tuples; returns the handle."""
+        arr = (MixedJob * len(jobs))(*[MixedJob(OP_CODES[op] if isinstance(op, str) else int(op), int(n), int(i),
+                                                int(o)) for op, n, i, o in jobs])
+        h = self.lib.minfft_b200_mixed_plan(len(jobs), arr)
+        if not h:
+            code = self.last_error()
+            raise MinfftError(code or 1, self.last_error_message())
+        return int(h)
+
+    def mixed_execute(self, handle: int, stream: int = 0) -> None:
+        if self.lib.minfft_b200_mixed_execute(ctypes.c_void_p(handle), ctypes.c_void_p(stream or None)):
+            self.check()
+
+    def mixed_autotune(self, handle: int, reps: int = 3) -> None:
+        if self.lib.minfft_b200_mixed_autotune(ctypes.c_void_p(handle), int(reps)):
+            self.check()
+
+    def mixed_items(self, handle: int) -> int:
+        return int(self.lib.minfft_b200_mixed_items(ctypes.c_void_p(handle)))
+
+    def mixed_free(self, handle: int) -> None:
+        self.lib.minfft_b200_mixed_free(ctypes.c_void_p(handle))
 
     # ---------------------------------------------- checked plan API
     def plan(self, family: str, dims: Sequence[int]) -> "Plan":
@@ -254,5 +295,5 @@ def transform(op: str, x, dims: Optional[Sequence[int]] = None, single: Optional
     return out
 
 
-__all__ = ["ERROR_NAMES", "Engine", "Plan", "MinfftError", "engine", "transform", "shapes", "OPS", "FAMILIES", "OP_FAMILY",
+__all__ = ["ERROR_NAMES", "MixedJob", "Engine", "Plan", "MinfftError", "engine", "transform", "shapes", "OPS", "FAMILIES", "OP_FAMILY",
            "OP_CODES", "LIB_PATHS"]

@@ -25,6 +25,14 @@ const void* axis_kernel(int combo, int log2L, int R = 16);
 // for log2(L) = 1 .. 13, or nullptr.
 const void* pipe_kernel(int combo, int log2L, int R = 16);
 
+// Root tables kept on the device by plans: w_N^m (m < N); the real-DFT
+// table w_N^k (k < N/4); the type-2/3 table w_4N^n (n < N/2); the type-4
+// tables w_2N^n (n < N/2) and w_8N^(2q+1) (q < N); and the coarse/fine pair
+// of a long length (w_N^(a << lobits), w_N^c), lobits = ceil(log2 N / 2).
+namespace tables {
+enum TableKind : int { TB_TW = 0, TB_RFT, TB_T23, TB_T4PRE, TB_T4POST, TB_STHI, TB_STLO };
+}
+
 // Radix actually used by a kernel of length L requested with radix R.
 inline int effective_radix(int L, int R) { return L < R ? L : R; }
 

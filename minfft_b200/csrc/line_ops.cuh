@@ -1,0 +1,258 @@
+// Element-wise pre- and post-processing steps of real-data transforms whose
+// half-length complex DFT runs as several HBM passes, and the length-1 axis
+// steps, as device functions: Op::count(p) work items, Op::item(p, e) does
+// item e.  Used by the line kernels (line_kernels.cu) and by the mixed-batch
+// kernel (mixed.cu).
+//
+// Data layout: a batch of outer x inner lines along one axis; element n of
+// line (o, i) of the input sits at o*in_so + n*in_sn + i, of the output at
+// o*out_so + n*out_sn + i.  The item index runs fastest over i (adjacent
+// columns) and then over n, so a warp touches contiguous memory for both
+// column and row layouts.
+#pragma once
+
+#include "axis_pass.cuh"
+#include "line_kernels.h"
+
+namespace mb {
+
+struct ItemIdx {
+  int64_t o, n, i;
+};
+
+__device__ __forceinline__ ItemIdx split_item(int64_t e, int64_t inner, int64_t K) {
+  ItemIdx r;
+  r.i = e % inner;
+  const int64_t q = e / inner;
+  r.n = q % K;
+  r.o = q / K;
+  return r;
+}
+
+// complex t_m = (u_2m, u_2m+1) of the type-2 permutation (see LoadDCT2)
+struct Op_dct2_pre {
+  static __device__ __forceinline__ int64_t count(const LineParams& p) {
+    const int64_t L = p.L, N = 2 * L;
+    const real sg = (p.flags & F_DST) ? real(-1) : real(1);
+    return p.outer * p.inner * L;
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const int64_t L = p.L, N = 2 * L;
+    const real sg = (p.flags & F_DST) ? real(-1) : real(1);
+    const ItemIdx it = split_item(e, p.inner, L);
+    const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
+    const int64_t i0 = 2 * it.n, i1 = 2 * it.n + 1;
+    const real a = i0 < L ? in[(2 * i0) * p.in_sn] : sg * in[(2 * N - 1 - 2 * i0) * p.in_sn];
+    const real b = i1 < L ? in[(2 * i1) * p.in_sn] : sg * in[(2 * N - 1 - 2 * i1) * p.in_sn];
+    static_cast<cpx*>(p.out)[it.o * p.out_so + it.n * p.out_sn + it.i] = cmk(a, b);
+  }
+};
+
+// type-4 pre-rotation (see LoadT4)
+struct Op_t4_pre {
+  static __device__ __forceinline__ int64_t count(const LineParams& p) {
+    const int64_t L = p.L, N = 2 * L;
+    const bool dst = (p.flags & F_DST) != 0;
+    return p.outer * p.inner * L;
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const int64_t L = p.L, N = 2 * L;
+    const bool dst = (p.flags & F_DST) != 0;
+    const ItemIdx it = split_item(e, p.inner, L);
+    const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
+    const real a = in[(2 * it.n) * p.in_sn];
+    const real b = in[(N - 1 - 2 * it.n) * p.in_sn];
+    const cpx w = ldg(p.t1 + it.n);
+    cpx v;
+    if (!dst) {
+      v = cmul(w, cmk(a, b));
+    } else {
+      const cpx q = cmul(w, cmk(a, -b));
+      v = cmk(-q.x, -q.y);
+    }
+    static_cast<cpx*>(p.out)[it.o * p.out_so + it.n * p.out_sn + it.i] = v;
+  }
+};
+
+// inverse-real-DFT packing, conjugated (see LoadC2R); in: L+1 spectrum values
+struct Op_c2r_pack {
+  static __device__ __forceinline__ int64_t count(const LineParams& p) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    return p.outer * p.inner * K;
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const ItemIdx it = split_item(e, p.inner, K);
+    const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
+    cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
+    const int64_t k = it.n;
+    const cpx z0 = in[k * p.in_sn], z1 = in[(L - k) * p.in_sn];
+    if (k == 0) {
+      out[0] = cmk(z0.x + z1.x, -(z0.x - z1.x));
+    } else if (2 * k == L) {
+      out[k * p.out_sn] = cmk(2 * z0.x, 2 * z0.y);
+    } else {
+      cpx ta, tb;
+      pack_pair(z0, z1, ldg(p.t2 + k), ta, tb);
+      out[k * p.out_sn] = cconj(ta);
+      out[(L - k) * p.out_sn] = cconj(tb);
+    }
+  }
+};
+
+// type-3 pre-rotation + packing, conjugated (see LoadDCT3)
+struct Op_dct3_pack {
+  static __device__ __forceinline__ int64_t count(const LineParams& p) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const bool dst = (p.flags & F_DST) != 0;
+    return p.outer * p.inner * K;
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const bool dst = (p.flags & F_DST) != 0;
+    const ItemIdx it = split_item(e, p.inner, K);
+    const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
+    cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
+    const int k = int(it.n);
+    const cpx z0 = LoadDCT3::zval(in, p.in_sn, k, int(L), dst, p.t1);
+    const cpx z1 = LoadDCT3::zval(in, p.in_sn, int(L) - k, int(L), dst, p.t1);
+    if (k == 0) {
+      out[0] = cmk(z0.x + z1.x, -(z0.x - z1.x));
+    } else if (2 * k == L) {
+      out[k * p.out_sn] = cmk(2 * z0.x, 2 * z0.y);
+    } else {
+      cpx ta, tb;
+      pack_pair(z0, z1, ldg(p.t2 + k), ta, tb);
+      out[k * p.out_sn] = cconj(ta);
+      out[(L - k) * p.out_sn] = cconj(tb);
+    }
+  }
+};
+
+// real-DFT unpacking (see StoreR2C); out: L+1 spectrum values
+struct Op_r2c_unpack {
+  static __device__ __forceinline__ int64_t count(const LineParams& p) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    return p.outer * p.inner * K;
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const ItemIdx it = split_item(e, p.inner, K);
+    const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
+    cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
+    const int64_t k = it.n;
+    const cpx za = in[k * p.in_sn];
+    if (k == 0) {
+      out[0] = cmk(za.x + za.y, real(0));
+      out[L * p.out_sn] = cmk(za.x - za.y, real(0));
+    } else if (2 * k == L) {
+      out[k * p.out_sn] = cconj(za);
+    } else {
+      cpx xa, xb;
+      unpack_pair(za, in[(L - k) * p.in_sn], ldg(p.t1 + k), xa, xb);
+      out[k * p.out_sn] = xa;
+      out[(L - k) * p.out_sn] = xb;
+    }
+  }
+};
+
+// type-2 unpacking + post-rotation (see StoreDCT2)
+struct Op_dct2_post {
+  static __device__ __forceinline__ int64_t count(const LineParams& p) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const int N = int(2 * L);
+    const bool dst = (p.flags & F_DST) != 0;
+    const real r2 = real(1.414213562373095048801688724209698079);
+    return p.outer * p.inner * K;
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const int N = int(2 * L);
+    const bool dst = (p.flags & F_DST) != 0;
+    const real r2 = real(1.414213562373095048801688724209698079);
+    const ItemIdx it = split_item(e, p.inner, K);
+    const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
+    real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
+    const int k = int(it.n);
+    const cpx za = in[k * p.in_sn];
+    if (k == 0) {
+      const real v0 = za.x + za.y, vl = za.x - za.y;
+      out[int64_t(dst ? N - 1 : 0) * p.out_sn] = 2 * v0;
+      out[int64_t(dst ? L - 1 : L) * p.out_sn] = r2 * vl;
+    } else if (2 * k == L) {
+      StoreDCT2::emit(out, p.out_sn, k, N, dst, cconj(za), ldg(p.t1 + k));
+    } else {
+      cpx xa, xb;
+      unpack_pair(za, in[(L - k) * p.in_sn], ldg(p.t2 + k), xa, xb);
+      StoreDCT2::emit(out, p.out_sn, k, N, dst, xa, ldg(p.t1 + k));
+      StoreDCT2::emit(out, p.out_sn, int(L) - k, N, dst, xb, ldg(p.t1 + (L - k)));
+    }
+  }
+};
+
+// type-3 de-interleave of the conjugated forward result (see StoreDCT3)
+struct Op_dct3_post {
+  static __device__ __forceinline__ int64_t count(const LineParams& p) {
+    const int64_t L = p.L, N = 2 * L;
+    const bool dst = (p.flags & F_DST) != 0;
+    return p.outer * p.inner * L;
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const int64_t L = p.L, N = 2 * L;
+    const bool dst = (p.flags & F_DST) != 0;
+    const ItemIdx it = split_item(e, p.inner, L);
+    const cpx w = cconj(static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i]);
+    real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
+    const int64_t i0 = 2 * it.n, i1 = 2 * it.n + 1;
+    const real a = (dst && i0 >= L) ? -w.x : w.x;
+    const real b = (dst && i1 >= L) ? -w.y : w.y;
+    out[(i0 < L ? 2 * i0 : 2 * N - 1 - 2 * i0) * p.out_sn] = a;
+    out[(i1 < L ? 2 * i1 : 2 * N - 1 - 2 * i1) * p.out_sn] = b;
+  }
+};
+
+// type-4 post-rotation (see StoreT4)
+struct Op_t4_post {
+  static __device__ __forceinline__ int64_t count(const LineParams& p) {
+    const int64_t L = p.L, N = 2 * L;
+    const bool dst = (p.flags & F_DST) != 0;
+    return p.outer * p.inner * L;
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const int64_t L = p.L, N = 2 * L;
+    const bool dst = (p.flags & F_DST) != 0;
+    const ItemIdx it = split_item(e, p.inner, L);
+    const cpx T = static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i];
+    real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
+    const int64_t m = it.n;
+    const cpx a = cmul(ldg(p.t2 + 2 * m), T);
+    const cpx b = cmul(ldg(p.t2 + (N - 1 - 2 * m)), cconj(T));
+    out[(2 * m) * p.out_sn] = 2 * (dst ? a.y : a.x);
+    out[(N - 1 - 2 * m) * p.out_sn] = 2 * (dst ? b.y : b.x);
+  }
+};
+
+// p.L = number of elements, p.flags selects the mode, p.scale the factor.
+struct Op_unit {
+  static __device__ __forceinline__ int64_t count(const LineParams& p) {
+    return p.L;
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    switch (p.mode) {
+      case UNIT_SCALE_REAL:
+        static_cast<real*>(p.out)[e] = p.scale * static_cast<const real*>(p.in)[e];
+        break;
+      case UNIT_REAL_TO_CPLX:
+        static_cast<cpx*>(p.out)[e] = cmk(static_cast<const real*>(p.in)[e], real(0));
+        break;
+      case UNIT_CPLX_TO_REAL:
+        static_cast<real*>(p.out)[e] = static_cast<const cpx*>(p.in)[e].x;
+        break;
+      default:
+        static_cast<cpx*>(p.out)[e] = static_cast<const cpx*>(p.in)[e];
+        break;
+    }
+  }
+};
+
+}  // namespace mb

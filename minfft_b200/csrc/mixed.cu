@@ -1,0 +1,721 @@
+// Mixed batches: thousands of independent 1-D transforms of any kind and
+// power-of-two length, run by one persistent kernel launched from a CUDA
+// graph.
+//
+// Planning (host).  Jobs are grouped by (kind, direction, length).  Each
+// group of transforms whose DFT fits in one CTA is cut into work items of up
+// to `cpb` transforms (the tile shape: the items of a length-L group use
+// L/16 threads per transform, so a 512-thread CTA holds 512*16/L of them);
+// every longer transform (64 K points at most) is one work item by itself.
+// Items are ordered by estimated cost, largest first, so the long ones start
+// early and the short ones fill the tail.
+//
+// Execution (device).  Every resident CTA takes the next item from an
+// atomic counter until the list is exhausted.  Short items run the same
+// load -> Stockham passes -> store code as the axis passes, with each
+// transform's own input and output pointers.  A long item is handled by its
+// CTA alone: the kind's element-wise pre-processing, two Stockham passes over
+// global memory through the CTA's private scratch slice (rounds of 32 or 64
+// sub-DFTs of 128/256 points), and the post-processing.
+//
+// No CTA ever waits on another (the queue is a single atomicAdd per item),
+// so the kernel cannot deadlock whatever the residency.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "kernel_registry.h"
+#include "line_ops.cuh"
+#include "minfft_b200.h"
+
+#define MB_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace mb {
+void set_last_error(int code, const char* msg);
+void host_table(int kind, int64_t N, std::vector<cpx>& h);
+}  // namespace mb
+
+namespace mb {
+namespace mixed {
+
+constexpr int kThreads = 512;
+constexpr int kSlots = 18;           // table slots by log2 length, 0 .. 17
+constexpr int kSmallMaxLog2L = 13;   // one-CTA DFTs up to 8192 points
+constexpr int kBigMaxLog2L = 16;     // two passes over global memory up to 65536
+constexpr int kOffsetsBytes = 1024;  // tile offsets of the long-item passes (<= 64 transforms)
+
+struct Job {
+  const void* in;
+  void* out;
+  int op;
+  int log2n;
+};
+
+// combo < 0: length-1 transforms (a scale or a type change per job)
+struct Item {
+  int combo;
+  int log2L;
+  int flags;
+  int count;
+  int first;  // index into the job order
+  int big;
+  int op;
+  int pad;
+};
+
+struct Params {
+  const Job* jobs;
+  const int* order;
+  const Item* items;
+  int nitems;
+  int pad;
+  unsigned* counter;
+  cpx* scratch;
+  int64_t scratch_stride;  // complex elements per CTA (two buffers)
+  const cpx* tw[kSlots];    // w_L^m, by log2 L
+  const cpx* rft[kSlots];   // real-DFT roots, by log2 N
+  const cpx* t23[kSlots];   // type-2/3 roots, by log2 N
+  const cpx* t4a[kSlots];   // type-4 pre-rotation, by log2 N
+  const cpx* t4b[kSlots];   // type-4 post-rotation, by log2 N
+  const cpx* sthi[kSlots];  // coarse roots of a long length, by log2 L
+  const cpx* stlo[kSlots];  // fine roots of a long length, by log2 L
+};
+
+__host__ __device__ constexpr int small_radix(int L) { return L < 16 ? L : 16; }
+__host__ __device__ constexpr int log2c(int v) { return v <= 1 ? 0 : 1 + log2c(v / 2); }
+__host__ __device__ constexpr int small_cpb(int L) { return kThreads / (L / small_radix(L)); }
+
+// ---------------------------------------------------------------- device
+template <int L, class LoadOp, class StoreOp>
+__device__ __noinline__ void run_small(const Params& mp, const Item& it, unsigned char* smem) {
+  constexpr int R = small_radix(L);
+  constexpr int TPT = L / R;
+  constexpr int CPB = kThreads / TPT;
+  const int c = threadIdx.x / TPT, j = threadIdx.x % TPT;
+  const bool active = c < it.count;
+  Job job{};
+  if (active) job = mp.jobs[mp.order[it.first + c]];
+  const int log2N = (it.combo == K_CPLX) ? it.log2L : it.log2L + 1;
+  AxisParams p;
+  memset(&p, 0, sizeof(p));
+  p.in = job.in;
+  p.out = job.out;
+  p.nbatch = it.count;
+  p.d0 = p.d1 = 1;
+  p.in_n = 1;
+  p.out_k = 1;
+  p.tw = mp.tw[it.log2L];
+  p.st_ns = 1;
+  p.st_div = 1;
+  p.cpb = CPB;
+  p.flags = it.flags;
+  p.lp = tile_pitch(L, R, CPB, 0);
+  switch (it.combo) {
+    case K_R2C:
+      p.t1 = mp.rft[log2N];
+      if ((reinterpret_cast<uintptr_t>(job.in) % sizeof(cpx)) == 0) p.flags |= F_VEC;
+      break;
+    case K_C2R:
+      p.t2 = mp.rft[log2N];
+      if ((reinterpret_cast<uintptr_t>(job.out) % sizeof(cpx)) == 0) p.flags |= F_VEC;
+      break;
+    case K_DCT2:
+    case K_DCT3:
+      p.t1 = mp.t23[log2N];
+      p.t2 = mp.rft[log2N];
+      break;
+    case K_T4:
+      p.t1 = mp.t4a[log2N];
+      p.t2 = mp.t4b[log2N];
+      break;
+    default: break;
+  }
+  Ctx x;
+  x.b = c;
+  x.b0 = 0;
+  x.oin = 0;
+  x.oout = 0;
+  x.c = c;
+  x.j = j;
+  x.active = active;
+  Tile t{reinterpret_cast<cpx*>(smem + kOffsetsBytes), p.lp};
+  TileOffsets to{nullptr, nullptr, it.count};
+  cpx v[R];
+  LoadOp::template run<L, R>(p, x, t, v);
+  run_passes<L, R, 1>(v, j, c, t, p.tw);
+  StoreOp::template run<L, R>(p, x, t, to, v);
+}
+
+// One Stockham pass over global memory of a long transform of length 2^LG,
+// sub-DFTs of length RP, span NS (1 or the length of the first pass).
+template <int LG, int RP, int NS>
+__device__ __forceinline__ void big_pass(const Params& mp, const cpx* src, cpx* dst, int flags,
+                                         unsigned char* smem) {
+  constexpr int Lc = 1 << LG;
+  constexpr int R = 16;
+  constexpr int TPT = RP / R;
+  constexpr int CPB = kThreads / TPT;
+  constexpr int NJ = Lc / RP;
+  static_assert(CPB * 2 * sizeof(int64_t) <= kOffsetsBytes, "offsets region");
+  AxisParams p;
+  memset(&p, 0, sizeof(p));
+  p.in = src;
+  p.out = dst;
+  p.nbatch = NJ;
+  p.d0 = NS;
+  p.d1 = Lc / (NS * RP);
+  p.is0 = 1;
+  p.is1 = NS;
+  p.is2 = Lc;
+  p.in_n = Lc / RP;
+  p.os0 = 1;
+  p.os1 = NS * RP;
+  p.os2 = Lc;
+  p.out_k = NS;
+  p.st_ns = NS;
+  p.st_div = 1;
+  p.st_shift = 0;
+  p.st_lobits = (LG + 1) / 2;
+  p.st_hi = mp.sthi[LG];
+  p.st_lo = mp.stlo[LG];
+  p.tw = mp.tw[log2c(RP)];
+  p.cpb = CPB;
+  p.colmode = 1;
+  p.flags = flags | (NS == 1 ? F_STAGE_ROWS : 0);
+  p.lp = tile_pitch(RP, R, CPB, 1);
+  int64_t* offs = reinterpret_cast<int64_t*>(smem);
+  Tile t{reinterpret_cast<cpx*>(smem + kOffsetsBytes), p.lp};
+  const int c = threadIdx.x % CPB, j = threadIdx.x / CPB;
+  for (int round = 0; round * CPB < NJ; ++round) {
+    const int64_t base = int64_t(round) * CPB;
+    if (threadIdx.x < CPB) {
+      int64_t b0, oi, oo;
+      batch_offsets(p, base + threadIdx.x < NJ ? base + threadIdx.x : 0, b0, oi, oo);
+      offs[threadIdx.x] = oi;
+      offs[CPB + threadIdx.x] = oo;
+    }
+    __syncthreads();
+    const int left = int(NJ - base);
+    TileOffsets to{offs, offs + CPB, left < CPB ? left : CPB};
+    Ctx x;
+    x.c = c;
+    x.j = j;
+    x.b = base + c;
+    x.active = x.b < NJ;
+    x.b0 = x.b % p.d0;
+    x.oin = offs[c];
+    x.oout = offs[CPB + c];
+    cpx v[R];
+    LoadCplx::template run<RP, R>(p, x, t, v);
+    run_passes<RP, R, 1>(v, j, c, t, p.tw);
+    StoreCplx::template run<RP, R>(p, x, t, to, v);
+    __syncthreads();
+  }
+}
+
+template <class Op>
+__device__ __forceinline__ void cta_line(const LineParams& lp) {
+  const int64_t total = Op::count(lp);
+  for (int64_t e = threadIdx.x; e < total; e += blockDim.x) Op::item(lp, e);
+}
+
+template <int LG>
+__device__ __noinline__ void run_big(const Params& mp, const Item& it, unsigned char* smem) {
+  constexpr int Lc = 1 << LG;
+  constexpr int B1 = (LG + 1) / 2, B2 = LG - B1;
+  constexpr int R1 = 1 << B1, R2 = 1 << B2;
+  const Job job = mp.jobs[mp.order[it.first]];
+  cpx* S1 = mp.scratch + int64_t(blockIdx.x) * mp.scratch_stride;
+  cpx* S2 = S1 + mp.scratch_stride / 2;
+  const int log2N = (it.combo == K_CPLX) ? LG : LG + 1;
+  LineParams lp;
+  memset(&lp, 0, sizeof(lp));
+  lp.outer = 1;
+  lp.inner = 1;
+  lp.L = Lc;
+  lp.in_sn = 1;
+  lp.out_sn = 1;
+  lp.flags = it.flags;
+  const cpx* src = static_cast<const cpx*>(job.in);
+  // element-wise pre-processing into S1 (real kinds whose input is not a complex view)
+  if (it.combo == K_C2R || it.combo == K_DCT2 || it.combo == K_DCT3 || it.combo == K_T4) {
+    lp.in = job.in;
+    lp.out = S1;
+    if (it.combo == K_C2R) {
+      lp.t2 = mp.rft[log2N];
+      cta_line<Op_c2r_pack>(lp);
+    } else if (it.combo == K_DCT2) {
+      cta_line<Op_dct2_pre>(lp);
+    } else if (it.combo == K_DCT3) {
+      lp.t1 = mp.t23[log2N];
+      lp.t2 = mp.rft[log2N];
+      cta_line<Op_dct3_pack>(lp);
+    } else {
+      lp.t1 = mp.t4a[log2N];
+      cta_line<Op_t4_pre>(lp);
+    }
+    src = S1;
+    __syncthreads();
+  }
+  cpx* mid = (src == S1) ? S2 : S1;
+  const bool inv_cplx = (it.combo == K_CPLX) && (it.flags & F_CONJ_IN);
+  big_pass<LG, R1, 1>(mp, src, mid, inv_cplx ? F_CONJ_IN : 0, smem);
+  __syncthreads();
+  const bool direct = (it.combo == K_CPLX || it.combo == K_C2R);
+  cpx* fin = direct ? static_cast<cpx*>(job.out) : (mid == S1 ? S2 : S1);
+  const bool conj_out = inv_cplx || it.combo == K_C2R;
+  big_pass<LG, R2, R1>(mp, mid, fin, conj_out ? F_CONJ_OUT : 0, smem);
+  __syncthreads();
+  if (!direct) {
+    lp.in = fin;
+    lp.out = job.out;
+    if (it.combo == K_R2C) {
+      lp.t1 = mp.rft[log2N];
+      cta_line<Op_r2c_unpack>(lp);
+    } else if (it.combo == K_DCT2) {
+      lp.t1 = mp.t23[log2N];
+      lp.t2 = mp.rft[log2N];
+      cta_line<Op_dct2_post>(lp);
+    } else if (it.combo == K_DCT3) {
+      cta_line<Op_dct3_post>(lp);
+    } else {
+      lp.t2 = mp.t4b[log2N];
+      cta_line<Op_t4_post>(lp);
+    }
+  }
+}
+
+// length-1 transforms: y = 2x (type 2), x (type 3), sqrt(2) x (type 4),
+// (x, 0) (real DFT), Re z (inverse real DFT), z (complex DFT)
+__device__ __noinline__ void run_unit(const Params& mp, const Item& it) {
+  for (int c = threadIdx.x; c < it.count; c += blockDim.x) {
+    const Job job = mp.jobs[mp.order[it.first + c]];
+    switch (job.op) {
+      case MINFFT_B200_DFT:
+      case MINFFT_B200_INVDFT: *static_cast<cpx*>(job.out) = *static_cast<const cpx*>(job.in); break;
+      case MINFFT_B200_REALDFT: *static_cast<cpx*>(job.out) = cmk(*static_cast<const real*>(job.in), real(0)); break;
+      case MINFFT_B200_INVREALDFT: *static_cast<real*>(job.out) = static_cast<const cpx*>(job.in)->x; break;
+      case MINFFT_B200_DCT2:
+      case MINFFT_B200_DST2: *static_cast<real*>(job.out) = 2 * *static_cast<const real*>(job.in); break;
+      case MINFFT_B200_DCT3:
+      case MINFFT_B200_DST3: *static_cast<real*>(job.out) = *static_cast<const real*>(job.in); break;
+      default:
+        *static_cast<real*>(job.out) = real(1.414213562373095048801688724209698079) * *static_cast<const real*>(job.in);
+        break;
+    }
+  }
+}
+
+template <class Ld, class St>
+__device__ __forceinline__ void run_small_any(const Params& mp, const Item& it, unsigned char* smem) {
+  switch (it.log2L) {
+    case 0: run_small<1, Ld, St>(mp, it, smem); break;
+    case 1: run_small<2, Ld, St>(mp, it, smem); break;
+    case 2: run_small<4, Ld, St>(mp, it, smem); break;
+    case 3: run_small<8, Ld, St>(mp, it, smem); break;
+    case 4: run_small<16, Ld, St>(mp, it, smem); break;
+    case 5: run_small<32, Ld, St>(mp, it, smem); break;
+    case 6: run_small<64, Ld, St>(mp, it, smem); break;
+    case 7: run_small<128, Ld, St>(mp, it, smem); break;
+    case 8: run_small<256, Ld, St>(mp, it, smem); break;
+    case 9: run_small<512, Ld, St>(mp, it, smem); break;
+    case 10: run_small<1024, Ld, St>(mp, it, smem); break;
+    case 11: run_small<2048, Ld, St>(mp, it, smem); break;
+    case 12: run_small<4096, Ld, St>(mp, it, smem); break;
+    case 13: run_small<8192, Ld, St>(mp, it, smem); break;
+    default: break;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, MinBlocks<16>::value) mixed_kernel(const __grid_constant__ Params mp) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = int(atomicAdd(mp.counter, 1u));
+    __syncthreads();
+    const int idx = s_item;
+    __syncthreads();
+    if (idx >= mp.nitems) break;
+    const Item it = mp.items[idx];
+    if (it.big) {
+      switch (it.log2L) {
+        case 14: run_big<14>(mp, it, smem); break;
+        case 15: run_big<15>(mp, it, smem); break;
+        case 16: run_big<16>(mp, it, smem); break;
+        default: break;
+      }
+    } else if (it.combo < 0) {
+      run_unit(mp, it);
+    } else {
+      switch (it.combo) {
+        case K_CPLX: run_small_any<LoadCplx, StoreCplx>(mp, it, smem); break;
+        case K_R2C: run_small_any<LoadR2C, StoreR2C>(mp, it, smem); break;
+        case K_C2R: run_small_any<LoadC2R, StoreC2R>(mp, it, smem); break;
+        case K_DCT2: run_small_any<LoadDCT2, StoreDCT2>(mp, it, smem); break;
+        case K_DCT3: run_small_any<LoadDCT3, StoreDCT3>(mp, it, smem); break;
+        default: run_small_any<LoadT4, StoreT4>(mp, it, smem); break;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// shared memory of the kernel: offsets + the largest tile of any item
+size_t kernel_smem() {
+  size_t m = 0;
+  for (int lg = 0; lg <= kSmallMaxLog2L; ++lg) {
+    const int L = 1 << lg;
+    const int cpb = small_cpb(L);
+    m = std::max(m, size_t(cpb) * tile_pitch(L, small_radix(L), cpb, 0) * sizeof(cpx));
+  }
+  for (int rp : {64, 128, 256}) {
+    const int cpb = kThreads / (rp / 16);
+    m = std::max(m, size_t(cpb) * tile_pitch(rp, 16, cpb, 1) * sizeof(cpx));
+  }
+  return kOffsetsBytes + 16 * ((m + 15) / 16);
+}
+
+}  // namespace mixed
+}  // namespace mb
+
+// ==================================================================== host
+using mb::cpx;
+using mb::real;
+using namespace mb::mixed;
+
+struct minfft_b200_mixed {
+  int device = 0;
+  int count = 0;
+  std::vector<Job> jobs;
+  std::vector<int> order;
+  std::vector<Item> items;
+  Params params;
+  void* d_jobs = nullptr;
+  void* d_order = nullptr;
+  void* d_items = nullptr;
+  unsigned* d_counter = nullptr;
+  cpx* d_scratch = nullptr;
+  std::vector<void*> tables;
+  int grid = 0;
+  int per_sm = 1;
+  size_t smem = 0;
+  int split = 1;  // jobs per short item = slots / split
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+bool ok(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  char buf[256];
+  snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  mb::set_last_error(e == cudaErrorMemoryAllocation ? MINFFT_B200_ENOMEM : MINFFT_B200_ECUDA, buf);
+  return false;
+}
+
+int fail(int code, const char* msg) {
+  mb::set_last_error(code, msg);
+  return code;
+}
+
+int ilog2i(int64_t v) {
+  int r = 0;
+  while ((int64_t(1) << r) < v) ++r;
+  return r;
+}
+
+int combo_of(int op) {
+  switch (op) {
+    case MINFFT_B200_DFT:
+    case MINFFT_B200_INVDFT: return mb::K_CPLX;
+    case MINFFT_B200_REALDFT: return mb::K_R2C;
+    case MINFFT_B200_INVREALDFT: return mb::K_C2R;
+    case MINFFT_B200_DCT2:
+    case MINFFT_B200_DST2: return mb::K_DCT2;
+    case MINFFT_B200_DCT3:
+    case MINFFT_B200_DST3: return mb::K_DCT3;
+    default: return mb::K_T4;
+  }
+}
+
+int flags_of(int op) {
+  if (op == MINFFT_B200_INVDFT) return mb::F_CONJ_IN | mb::F_CONJ_OUT;
+  if (op == MINFFT_B200_DST2 || op == MINFFT_B200_DST3 || op == MINFFT_B200_DST4) return mb::F_DST;
+  return 0;
+}
+
+const cpx* upload(minfft_b200_mixed* m, int kind, int64_t N) {
+  std::vector<cpx> h;
+  mb::host_table(kind, N, h);
+  void* d = nullptr;
+  if (!ok(cudaMalloc(&d, h.size() * sizeof(cpx)), "cudaMalloc(table)")) return nullptr;
+  m->tables.push_back(d);
+  if (!ok(cudaMemcpy(d, h.data(), h.size() * sizeof(cpx), cudaMemcpyHostToDevice), "cudaMemcpy(table)"))
+    return nullptr;
+  return static_cast<const cpx*>(d);
+}
+
+void release_graph(minfft_b200_mixed* m) {
+  if (m->exec) cudaGraphExecDestroy(m->exec);
+  if (m->graph) cudaGraphDestroy(m->graph);
+  m->exec = nullptr;
+  m->graph = nullptr;
+}
+
+// Cut the job groups into items (short groups: slots/split jobs per item),
+// order them by cost, upload, and capture counter reset + kernel in a graph.
+bool build_items(minfft_b200_mixed* m) {
+  std::map<std::tuple<int, int, int, int>, std::vector<int>> groups;  // (big, combo, flags, log2L) -> jobs
+  for (int i = 0; i < m->count; ++i) {
+    const Job& j = m->jobs[i];
+    const int combo = combo_of(j.op);
+    const int64_t n = int64_t(1) << j.log2n;
+    if (n == 1) {
+      groups[std::make_tuple(0, -1, 0, 0)].push_back(i);
+      continue;
+    }
+    const int lgL = combo == mb::K_CPLX ? j.log2n : j.log2n - 1;
+    groups[std::make_tuple(lgL > kSmallMaxLog2L ? 1 : 0, combo, flags_of(j.op), lgL)].push_back(i);
+  }
+  std::vector<std::pair<double, Item>> its;
+  m->order.clear();
+  for (auto& g : groups) {
+    const int big = std::get<0>(g.first), combo = std::get<1>(g.first), flags = std::get<2>(g.first),
+              lgL = std::get<3>(g.first);
+    const std::vector<int>& js = g.second;
+    const int L = 1 << lgL;
+    int per = big ? 1 : (combo < 0 ? kThreads : std::max(1, small_cpb(L) / m->split));
+    for (size_t s = 0; s < js.size(); s += per) {
+      Item it{};
+      it.combo = combo;
+      it.log2L = lgL;
+      it.flags = flags;
+      it.count = int(std::min<size_t>(per, js.size() - s));
+      it.first = int(m->order.size());
+      it.big = big;
+      it.op = m->jobs[js[s]].op;
+      for (int k = 0; k < it.count; ++k) m->order.push_back(js[s + k]);
+      // cost: points processed (x2 passes and pre/post for the long ones)
+      const double cost = double(L) * std::max(1, lgL) * (big ? 3.0 : 1.0) * (big ? 1 : it.count);
+      its.push_back(std::make_pair(cost, it));
+    }
+  }
+  std::stable_sort(its.begin(), its.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  m->items.clear();
+  for (auto& p : its) m->items.push_back(p.second);
+  if (m->d_order) cudaFree(m->d_order);
+  if (m->d_items) cudaFree(m->d_items);
+  m->d_order = m->d_items = nullptr;
+  if (!ok(cudaMalloc(&m->d_order, std::max<size_t>(1, m->order.size()) * sizeof(int)), "cudaMalloc(order)") ||
+      !ok(cudaMalloc(&m->d_items, std::max<size_t>(1, m->items.size()) * sizeof(Item)), "cudaMalloc(items)"))
+    return false;
+  if (!m->order.empty() &&
+      !ok(cudaMemcpy(m->d_order, m->order.data(), m->order.size() * sizeof(int), cudaMemcpyHostToDevice),
+          "cudaMemcpy(order)"))
+    return false;
+  if (!m->items.empty() &&
+      !ok(cudaMemcpy(m->d_items, m->items.data(), m->items.size() * sizeof(Item), cudaMemcpyHostToDevice),
+          "cudaMemcpy(items)"))
+    return false;
+  m->params.order = static_cast<const int*>(m->d_order);
+  m->params.items = static_cast<const Item*>(m->d_items);
+  m->params.nitems = int(m->items.size());
+  // graph: reset the queue counter, run the persistent kernel
+  release_graph(m);
+  cudaStream_t cs;
+  if (!ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
+  bool good = ok(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  if (good) {
+    cudaMemsetAsync(m->d_counter, 0, sizeof(unsigned), cs);
+    void* args[1] = {&m->params};
+    cudaLaunchKernel((const void*)mixed_kernel, dim3(m->grid), dim3(kThreads), args, m->smem, cs);
+    good = ok(cudaStreamEndCapture(cs, &m->graph), "cudaStreamEndCapture");
+  }
+  if (good) good = ok(cudaGraphInstantiate(&m->exec, m->graph, 0), "cudaGraphInstantiate");
+  cudaStreamDestroy(cs);
+  return good;
+}
+
+}  // namespace
+
+MB_EXPORT void minfft_b200_mixed_free(minfft_b200_mixed* m) {
+  if (!m) return;
+  release_graph(m);
+  for (void* t : m->tables) cudaFree(t);
+  cudaFree(m->d_jobs);
+  cudaFree(m->d_order);
+  cudaFree(m->d_items);
+  cudaFree(m->d_counter);
+  cudaFree(m->d_scratch);
+  delete m;
+}
+
+MB_EXPORT minfft_b200_mixed* minfft_b200_mixed_plan(int count, const minfft_b200_job* jobs) {
+  if (count < 1 || !jobs) {
+    fail(MINFFT_B200_EINVAL, "mixed plan: need at least one job");
+    return nullptr;
+  }
+  minfft_b200_mixed* m = new (std::nothrow) minfft_b200_mixed();
+  if (!m) {
+    fail(MINFFT_B200_ENOMEM, "mixed plan: host allocation failed");
+    return nullptr;
+  }
+  m->count = count;
+  m->jobs.resize(count);
+  int max_big = 0;
+  std::vector<int> need_tw(kSlots, 0), need_n(kSlots, 0), need_st(kSlots, 0);
+  std::vector<int> need_kind(kSlots * 8, 0);
+  for (int i = 0; i < count; ++i) {
+    const minfft_b200_job& j = jobs[i];
+    const int64_t n = j.n;
+    if (j.op < MINFFT_B200_DFT || j.op > MINFFT_B200_DST4 || n < 1 || (n & (n - 1)) || !j.in || !j.out) {
+      char buf[160];
+      snprintf(buf, sizeof(buf), "mixed plan: job %d has a bad transform code, length or pointer", i);
+      fail(MINFFT_B200_EINVAL, buf);
+      minfft_b200_mixed_free(m);
+      return nullptr;
+    }
+    const int combo = combo_of(j.op);
+    const int lgn = ilog2i(n);
+    const int lgL = (combo == mb::K_CPLX) ? lgn : std::max(lgn - 1, 0);
+    if (lgL > kBigMaxLog2L) {
+      fail(MINFFT_B200_EINVAL, "mixed plan: lengths above 65536 complex points (131072 real) are not supported");
+      minfft_b200_mixed_free(m);
+      return nullptr;
+    }
+    // complex arrays are accessed as aligned pairs; so are the real arrays a
+    // long real DFT reads (or a long inverse writes) as complex values
+    const bool cin = combo == mb::K_CPLX || combo == mb::K_C2R || (combo == mb::K_R2C && lgL > kSmallMaxLog2L);
+    const bool cout = combo == mb::K_CPLX || combo == mb::K_R2C || (combo == mb::K_C2R && lgL > kSmallMaxLog2L);
+    if ((cin && reinterpret_cast<uintptr_t>(j.in) % sizeof(cpx)) ||
+        (cout && reinterpret_cast<uintptr_t>(j.out) % sizeof(cpx))) {
+      fail(MINFFT_B200_EINVAL, "mixed plan: complex data must be aligned to its size");
+      minfft_b200_mixed_free(m);
+      return nullptr;
+    }
+    m->jobs[i] = Job{j.in, j.out, j.op, lgn};
+    if (n == 1) continue;
+    if (lgL > kSmallMaxLog2L) {
+      max_big = std::max(max_big, lgL);
+      need_st[lgL] = 1;
+      need_tw[(lgL + 1) / 2] = 1;
+      need_tw[lgL - (lgL + 1) / 2] = 1;
+    } else {
+      need_tw[lgL] = 1;
+    }
+    need_kind[combo * kSlots + lgn] = 1;
+  }
+  if (!ok(cudaGetDevice(&m->device), "cudaGetDevice")) {
+    minfft_b200_mixed_free(m);
+    return nullptr;
+  }
+  Params& P = m->params;
+  memset(&P, 0, sizeof(P));
+  bool good = true;
+  for (int lg = 0; lg < kSlots && good; ++lg) {
+    const int64_t L = int64_t(1) << lg;
+    if (need_tw[lg]) good = (P.tw[lg] = upload(m, mb::tables::TB_TW, L)) != nullptr;
+    if (good && need_st[lg]) {
+      good = (P.sthi[lg] = upload(m, mb::tables::TB_STHI, L)) && (P.stlo[lg] = upload(m, mb::tables::TB_STLO, L));
+    }
+    for (int combo = 1; combo < mb::K_COUNT && good; ++combo) {
+      if (!need_kind[combo * kSlots + lg]) continue;
+      const int64_t N = L;
+      if (combo == mb::K_R2C || combo == mb::K_C2R || combo == mb::K_DCT2 || combo == mb::K_DCT3)
+        if (!P.rft[lg]) good = (P.rft[lg] = upload(m, mb::tables::TB_RFT, N)) != nullptr;
+      if (good && (combo == mb::K_DCT2 || combo == mb::K_DCT3) && !P.t23[lg])
+        good = (P.t23[lg] = upload(m, mb::tables::TB_T23, N)) != nullptr;
+      if (good && combo == mb::K_T4 && !P.t4a[lg])
+        good = (P.t4a[lg] = upload(m, mb::tables::TB_T4PRE, N)) && (P.t4b[lg] = upload(m, mb::tables::TB_T4POST, N));
+    }
+  }
+  int sms = 148;
+  if (good) good = ok(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device), "device query");
+  m->smem = kernel_smem();
+  if (good)
+    good = ok(cudaFuncSetAttribute((const void*)mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(m->smem)),
+              "cudaFuncSetAttribute");
+  int occ = 1;
+  if (good)
+    good = ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)mixed_kernel, kThreads, m->smem),
+              "occupancy query");
+  m->per_sm = std::max(1, occ);
+  m->grid = sms * m->per_sm;
+  if (good) good = ok(cudaMalloc(&m->d_jobs, count * sizeof(Job)), "cudaMalloc(jobs)");
+  if (good)
+    good = ok(cudaMemcpy(m->d_jobs, m->jobs.data(), count * sizeof(Job), cudaMemcpyHostToDevice), "cudaMemcpy(jobs)");
+  if (good) good = ok(cudaMalloc(&m->d_counter, sizeof(unsigned)), "cudaMalloc(counter)");
+  if (good && max_big > 0) {
+    P.scratch_stride = int64_t(2) << kBigMaxLog2L;
+    good = ok(cudaMalloc(&m->d_scratch, size_t(m->grid) * P.scratch_stride * sizeof(cpx)), "cudaMalloc(scratch)");
+  }
+  P.jobs = static_cast<const Job*>(m->d_jobs);
+  P.counter = m->d_counter;
+  P.scratch = m->d_scratch;
+  if (good) good = build_items(m);
+  if (!good) {
+    minfft_b200_mixed_free(m);
+    return nullptr;
+  }
+  return m;
+}
+
+MB_EXPORT int minfft_b200_mixed_execute(minfft_b200_mixed* m, void* stream) {
+  if (!m || !m->exec) return fail(MINFFT_B200_EINVAL, "mixed execute: NULL plan");
+  return ok(cudaGraphLaunch(m->exec, static_cast<cudaStream_t>(stream)), "cudaGraphLaunch") ? MINFFT_B200_OK
+                                                                                             : MINFFT_B200_ECUDA;
+}
+
+MB_EXPORT int minfft_b200_mixed_items(const minfft_b200_mixed* m) { return m ? int(m->items.size()) : -1; }
+
+// Time the plan's tile shapes (jobs per short work item: all slots, 1/2,
+// 1/4, 1/8 of them) and persistent grid sizes (1 .. max CTAs per SM), keep
+// the fastest.  Runs the batch several times (outputs are overwritten).
+MB_EXPORT int minfft_b200_mixed_autotune(minfft_b200_mixed* m, int reps) {
+  if (!m) return fail(MINFFT_B200_EINVAL, "mixed autotune: NULL plan");
+  if (reps < 1) reps = 3;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
+  const int max_per_sm = m->per_sm;
+  cudaStream_t st;
+  if (!ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate")) return MINFFT_B200_ECUDA;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int best_split = m->split, best_per = m->per_sm;
+  const int grid_cap = m->grid;  // scratch is sized for this many CTAs
+  for (int split : {1, 2, 4, 8}) {
+    for (int per = 1; per <= max_per_sm; ++per) {
+      m->split = split;
+      m->grid = std::min(grid_cap, sms * per);
+      if (!build_items(m)) continue;
+      cudaGraphLaunch(m->exec, st);
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < reps; ++r) cudaGraphLaunch(m->exec, st);
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms > 0 && ms < best) {
+        best = ms;
+        best_split = split;
+        best_per = per;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  m->split = best_split;
+  m->grid = std::min(grid_cap, sms * best_per);
+  return build_items(m) ? MINFFT_B200_OK : MINFFT_B200_ECUDA;
+}

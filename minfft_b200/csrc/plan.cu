@@ -258,8 +258,7 @@ int op_family(int op) {
   }
 }
 
-// table kinds kept on the device by each plan
-enum TableKind : int { TB_TW = 0, TB_RFT, TB_T23, TB_T4PRE, TB_T4POST, TB_STHI, TB_STLO };
+using namespace mb::tables;
 
 }  // namespace
 
@@ -302,18 +301,12 @@ namespace {
 
 int64_t st_lobits_for(int64_t Lt) { return (ilog2(Lt) + 1) / 2; }
 
-// Device table of the given kind for length N (built on first use).
-const cpx* table(minfft_aux* a, int kind, int64_t N) {
-  auto key = std::make_pair(kind, N);
-  auto it = a->tables.find(key);
-  if (it != a->tables.end()) return static_cast<const cpx*>(it->second);
-  if (a->host_only) {
-    // placeholder address: self-check plans are never executed
-    static cpx dummy[1];
-    a->tables[key] = dummy;
-    return dummy;
-  }
-  std::vector<cpx> h;
+}  // namespace
+
+namespace mb {
+// Host values of root table `kind` for length N (see TableKind).
+void host_table(int kind, int64_t N, std::vector<cpx>& h) {
+  h.clear();
   switch (kind) {
     case TB_TW:  // w_N^m, m < N
       h.resize(N);
@@ -347,8 +340,27 @@ const cpx* table(minfft_aux* a, int kind, int64_t N) {
       for (int64_t q = 0; q < (int64_t)h.size(); ++q) h[q] = root_w(q, N);
       break;
     }
-    default: return nullptr;
+    default: break;
   }
+}
+}  // namespace mb
+
+namespace {
+
+// Device table of the given kind for length N (built on first use).
+const cpx* table(minfft_aux* a, int kind, int64_t N) {
+  auto key = std::make_pair(kind, N);
+  auto it = a->tables.find(key);
+  if (it != a->tables.end()) return static_cast<const cpx*>(it->second);
+  if (a->host_only) {
+    // placeholder address: self-check plans are never executed
+    static cpx dummy[1];
+    a->tables[key] = dummy;
+    return dummy;
+  }
+  std::vector<cpx> h;
+  mb::host_table(kind, N, h);
+  if (h.empty()) return nullptr;
   void* d = nullptr;
   const size_t bytes = h.size() * sizeof(cpx);
   if (!cuda_ok(cudaMalloc(&d, bytes), "cudaMalloc(table)")) return nullptr;
