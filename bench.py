@@ -126,6 +126,7 @@ class Workload2D:
     name = "2d2048"
     dims = (2048, 2048)
     nsets = 4
+    dtype = "f64+f32"
 
     def __init__(self, torch, dev):
         import minfft_b200
@@ -222,6 +223,14 @@ class Workload2D:
     cpu_sequences = (("realdft", ("realdft", "invrealdft"), False), ("t2t3", ("dct2", "dct3"), False),
                      ("realdft", ("realdft", "invrealdft"), True), ("t2t3", ("dct2", "dct3"), True))
 
+    @classmethod
+    def cpu_measure(cls, kind, threads, warm, reps):
+        """Seconds and flops of `reps` steps on the CPU: `threads` independent
+        instances of the step, one per OpenMP thread, each with its own plans."""
+        t = cpu_run(kind, cls.cpu_sequences, cls.dims, threads, threads, reps, warm)
+        n = int(np.prod(cls.dims))
+        return t, 2.5 * n * math.log2(n) * 8 * threads * reps
+
 
 class WorkloadBatch4096:
     """1024 independent complex DFTs of length 4096 (c128), forward then inverse."""
@@ -229,6 +238,7 @@ class WorkloadBatch4096:
     name = "batch4096"
     n, howmany = 4096, 1024
     nsets = 4
+    dtype = "f64"
 
     def __init__(self, torch, dev):
         import minfft_b200
@@ -288,7 +298,116 @@ class WorkloadBatch4096:
     cpu_sequences = None
 
 
-WORKLOADS = {"2d2048": Workload2D, "batch4096": WorkloadBatch4096}
+class WorkloadMixed:
+    """20000 independent 1-D transforms in one persistent graph-launched kernel:
+    log2 n uniform in 4..16, kinds uniform over dft, realdft, dct2, dst2,
+    dct3, dst3, dct4, dst4, float32, standard-normal inputs."""
+
+    name = "mixed20000"
+    count = 20000
+    kinds = ("dft", "realdft", "dct2", "dst2", "dct3", "dst3", "dct4", "dst4")
+    dtype = "f32"
+
+    @classmethod
+    def job_list(cls):
+        rng = np.random.default_rng(4)
+        ops = [cls.kinds[k] for k in rng.integers(0, len(cls.kinds), cls.count)]
+        ns = [1 << int(v) for v in rng.integers(4, 17, cls.count)]
+        return ops, ns
+
+    @classmethod
+    def cpu_measure(cls, kind, threads, warm, reps):
+        """Seconds and flops of `reps` sweeps of the batch on the CPU: every
+        (kind, n) group as one OpenMP batch of the reference library."""
+        ops, ns = cls.job_list()
+        groups = {}
+        for op, n in zip(ops, ns):
+            groups[(op, n)] = groups.get((op, n), 0) + 1
+        fam = {"dft": "dft", "realdft": "realdft", "dct4": "t4", "dst4": "t4"}
+        t = 0.0
+        for (op, n), cnt in sorted(groups.items()):
+            t += cpu_run(kind, ((fam.get(op, "t2t3"), (op,), True),), (n,), cnt, threads, reps, warm)
+        flops = sum((5.0 if op == "dft" else 2.5) * n * math.log2(n) for op, n in zip(ops, ns)) * reps
+        return t, flops
+
+    def __init__(self, torch, dev):
+        import minfft_b200
+        from minfft_b200 import shapes
+
+        self.torch = torch
+        self.ops, self.ns = self.job_list()
+        self.eng = minfft_b200.engine(True)
+        esz = 4
+        offs_in, offs_out, tot = [], [], 0
+        self.in_bytes = self.out_bytes = 0
+        for op, n in zip(self.ops, self.ns):
+            ins, inc, outs, outc = shapes(op, (n,))
+            bi = int(np.prod(ins)) * esz * (2 if inc else 1)
+            bo = int(np.prod(outs)) * esz * (2 if outc else 1)
+            offs_in.append((tot, bi))
+            tot += (bi + 255) // 256 * 256
+            offs_out.append((tot, bo))
+            tot += (bo + 255) // 256 * 256
+            self.in_bytes += bi
+            self.out_bytes += bo
+        self.pool = torch.empty(tot // 4 + 64, dtype=torch.float32, device=dev)
+        self.pool.normal_(generator=torch.Generator(device=dev).manual_seed(4))
+        base = self.pool.data_ptr()
+        self.jobs = [(op, n, base + oi, base + oo) for op, n, (oi, _), (oo, _) in zip(self.ops, self.ns, offs_in,
+                                                                                       offs_out)]
+        self.offs_in, self.offs_out = offs_in, offs_out
+        self.handle = self.eng.mixed_plan(self.jobs)
+        self.flops_per_transform = sum((5.0 if op == "dft" else 2.5) * n * math.log2(n)
+                                       for op, n in zip(self.ops, self.ns))
+        self.ops_per_step = 1
+
+    def plans(self):
+        return iter(())
+
+    @staticmethod
+    def cpu_sample(P):
+        return f"the whole 20000-transform batch once, each (kind, n) group as an OpenMP batch on {P} threads"
+
+    def tune(self):
+        self.eng.mixed_autotune(self.handle, 3)
+        return self.eng.mixed_items(self.handle)
+
+    def step(self, k):
+        self.eng.mixed_execute(self.handle)
+
+    def check_errors(self):
+        self.eng.check()
+
+    def launches_per_step(self):
+        return 1
+
+    def e2e_setup(self):
+        t = self.torch
+        self.hpool = t.empty(self.pool.shape, dtype=t.float32, pin_memory=True)
+        self.hpool.copy_(self.pool.cpu())
+        nb = self.pool.numel() * 4  # the whole pool (inputs and outputs) goes each way
+        return nb, nb
+
+    def e2e_step(self):
+        # inputs in, one graph launch, outputs back (pinned host pool)
+        self.pool.copy_(self.hpool, non_blocking=True)
+        self.eng.mixed_execute(self.handle)
+        self.hpool.copy_(self.pool, non_blocking=True)
+        self.torch.cuda.synchronize()
+
+    def config(self):
+        return {"workload": "20000 mixed 1-D transforms, one persistent graph-launched kernel",
+                "count": self.count, "log2n": "uniform integer 4..16", "kinds": list(self.kinds),
+                "precision": "f32", "flops": "5*N*log2(N) dft, 2.5*N*log2(N) real-data kinds",
+                "inputs": "standard normal (torch generator seed 4)",
+                "bytes_in_out": self.in_bytes + self.out_bytes,
+                "l2": "inputs and outputs total ~%.1f GB, far beyond the 126 MB L2" % ((self.in_bytes + self.out_bytes)
+                                                                                   / 1e9)}
+
+    cpu_sequences = ()
+
+
+WORKLOADS = {"2d2048": Workload2D, "batch4096": WorkloadBatch4096, "mixed20000": WorkloadMixed}
 
 
 # -------------------------------------------------------------- CPU timing
@@ -341,29 +460,32 @@ def run_reference(args):
     if rank != 0:
         return 0
     W = WORKLOADS[args.workload]
-    if W.cpu_sequences is None:
-        print(json.dumps({"impl": "reference", "unavailable": f"no CPU sequence defined for workload {W.name}"}))
+    if not hasattr(W, "cpu_measure"):
+        print(json.dumps({"impl": "reference", "unavailable": f"no CPU reference defined for workload {W.name}"}))
         return 0
     kind = cpu_kind()
     P = cpu_threads()
-    n = int(np.prod(W.dims))
-    flops_step = 2.5 * n * math.log2(n) * 8
-    t = cpu_run(kind, W.cpu_sequences, W.dims, P, P, reps=args.steps, warm=args.warmup)
-    value = flops_step * P * args.steps / t / 1e9
+    t, flops = W.cpu_measure(kind, P, args.warmup, args.steps)
+    value = flops / t / 1e9
     line = {"metric": "GFLOP/s (5N log2N complex, 2.5N log2N real-data)", "value": round(value, 3),
             "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1000 * t / args.steps, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": W.dtype, "data": "synthetic",
             "config": _ref_config(W), "impl": "reference",
             "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": P, "kind": kind,
-                             "sample": f"{P} concurrent independent instances of the step (one per thread, "
-                                       f"own plans), per timed step"},
+                             "sample": W.cpu_sample(P) if hasattr(W, "cpu_sample") else
+                             f"{P} concurrent independent instances of the step (one per thread, own plans), "
+                             f"per timed step"},
             "e2e": {"value": round(value, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
 
 def _ref_config(W):
+    if W.name == "mixed20000":
+        return {"workload": "20000 mixed 1-D transforms", "count": W.count, "log2n": "uniform integer 4..16",
+                "kinds": list(W.kinds), "precision": "f32",
+                "flops": "5*N*log2(N) dft, 2.5*N*log2(N) real-data kinds"}
     cfg = {"workload": "2-D realdft->invrealdft and dct2->dct3 round trips, 2048x2048, f64 and f32",
            "dims": list(W.dims), "precisions": ["f64", "f32"], "transforms_per_step": 8,
            "flops": "2.5*N*log2(N) per transform, N=2^22"}
@@ -400,6 +522,8 @@ def run_engine(args):
             for op in ops:
                 eng.autotune(plan.aux, op, getattr(W, "howmany_for", lambda o: 1)(op), 5)
             tuned = max(tuned, eng.tune_size())
+        if hasattr(W, "tune"):
+            tuned = W.tune()
         if args.tune_file:
             for eng, plan, ops in W.plans():
                 eng.tune_save(f"{args.tune_file}.{'f32' if eng.single else 'f64'}")
@@ -494,19 +618,20 @@ def run_engine(args):
 
     # CPU baseline (rank 0, one GPU only): the reference on the host cores
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu and W.cpu_sequences is not None:
+    if rank == 0 and world == 1 and not args.no_cpu and hasattr(W, "cpu_measure"):
         P = cpu_threads()
         kind = cpu_kind()
-        t = cpu_run(kind, W.cpu_sequences, W.dims, P, P, 1)
-        cpu = {"value": round(flops_step * P / t / 1e9, 3), "unit": "GFLOP/s", "cores": P, "kind": kind,
-               "sample": f"{P} concurrent independent instances of one step (one per OpenMP thread, own plans), "
-                         f"{t:.1f} s"}
+        t, flops = W.cpu_measure(kind, P, 1, 1)
+        cpu = {"value": round(flops / t / 1e9, 3), "unit": "GFLOP/s", "cores": P, "kind": kind,
+               "sample": (W.cpu_sample(P) if hasattr(W, "cpu_sample") else
+                          f"{P} concurrent independent instances of one step (one per OpenMP thread, own plans)")
+               + f", {t:.1f} s"}
 
     if rank == 0:
         line = {"metric": "GFLOP/s (5N log2N complex, 2.5N log2N real-data)", "value": round(value, 3),
                 "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64+f32" if args.workload == "2d2048" else "f64",
+                "vs_baseline": None, "dtype": W.dtype,
                 "data": "synthetic", "config": W.config(), "parallelism": f"replicas x{world}",
                 "gpu_launches": int(launches_per_step * args.steps), "clocks": clocks.summary(),
                 "autotuned_launch_configs": tuned,
