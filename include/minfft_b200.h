@@ -131,6 +131,31 @@ int minfft_b200_mixed_autotune(minfft_b200_mixed *m, int reps);
 int minfft_b200_mixed_items(const minfft_b200_mixed *m);
 void minfft_b200_mixed_free(minfft_b200_mixed *m);
 
+/* ----------------------------------------------- tensor-core precision */
+/* Arithmetic of plan `a`'s complex 256-point axis passes (single-precision
+ * library; no counterpart in the reference, whose arithmetic is its
+ * `minfft_real` type, minfft.h:14-31):
+ *   MINFFT_B200_PREC_FP32     FP32 on the CUDA cores (default);
+ *   MINFFT_B200_PREC_TC_F16   radix-16 stages as DFT-matrix contractions on
+ *                             the tensor cores, each row block-scaled by a
+ *                             power of two and split into two FP16 terms
+ *                             (three products, FP32 accumulation);
+ *   MINFFT_B200_PREC_TC_BF16  the same with three BF16 terms (six products).
+ * Every other axis keeps its FP32 kernels.  The double-precision library
+ * accepts only MINFFT_B200_PREC_FP32 (MINFFT_B200_EUNSUPPORTED otherwise).
+ * Applies to launch lists built afterwards (the plan's lists are rebuilt). */
+enum {
+    MINFFT_B200_PREC_FP32 = 0,
+    MINFFT_B200_PREC_TC_F16 = 1,
+    MINFFT_B200_PREC_TC_BF16 = 2
+};
+int minfft_b200_set_precision(minfft_aux *a, int mode);
+int minfft_b200_get_precision(const minfft_aux *a);
+/* Waits for plan `a`'s stream and reports whether a tensor-core pass gave up
+ * waiting for its matrix units (MINFFT_B200_ETIMEOUT; that pass's output is
+ * then incomplete) since the previous call; clears the record. */
+int minfft_b200_tc_status(const minfft_aux *a);
+
 /* ------------------------------------------------------------- autotuner */
 /* Time the candidate launch configurations (kernel form: one tile per CTA
  * or persistent CTAs with double-buffered asynchronous copies; per-thread
@@ -159,6 +184,9 @@ int minfft_b200_tune_set_default(int pipe, int cpb, int radix);
  * description, `launches` the launch count. */
 int minfft_b200_plan_selfcheck(int op, int d, const int *Ns, int howmany, int alias, char *report, int report_len,
                                int *launches);
+/* The same for a plan in arithmetic mode `precision` (MINFFT_B200_PREC_*). */
+int minfft_b200_plan_selfcheck_precision(int op, int d, const int *Ns, int howmany, int alias, int precision,
+                                         char *report, int report_len, int *launches);
 
 #ifdef __cplusplus
 } /* extern "C" */

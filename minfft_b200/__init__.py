@@ -26,6 +26,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 LIB_PATHS = {False: os.path.join(LIB_DIR, "libminfft_b200.so"), True: os.path.join(LIB_DIR, "libminfft_b200_single.so")}
 OP_CODES = {name: i for i, name in enumerate(OPS)}
 
+PRECISIONS = {"fp32": 0, "tc_f16": 1, "tc_bf16": 2}  # minfft_b200.h MINFFT_B200_PREC_*
 ERROR_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "EUNSUPPORTED", 5: "ETIMEOUT"}
 
 
@@ -79,6 +80,15 @@ class Engine(MinfftLibrary):
         L.minfft_b200_plan_selfcheck.argtypes = [i32, i32, ctypes.POINTER(i32), i32, i32, ctypes.c_char_p, i32,
                                                  ctypes.POINTER(i32)]
         L.minfft_b200_plan_selfcheck.restype = i32
+        L.minfft_b200_plan_selfcheck_precision.argtypes = [i32, i32, ctypes.POINTER(i32), i32, i32, i32,
+                                                           ctypes.c_char_p, i32, ctypes.POINTER(i32)]
+        L.minfft_b200_plan_selfcheck_precision.restype = i32
+        L.minfft_b200_set_precision.argtypes = [vp, i32]
+        L.minfft_b200_set_precision.restype = i32
+        L.minfft_b200_get_precision.argtypes = [vp]
+        L.minfft_b200_get_precision.restype = i32
+        L.minfft_b200_tc_status.argtypes = [vp]
+        L.minfft_b200_tc_status.restype = i32
         L.minfft_b200_autotune.argtypes = [vp, i32, i32, i32]
         L.minfft_b200_autotune.restype = i32
         for f in ("minfft_b200_tune_save", "minfft_b200_tune_load"):
@@ -135,14 +145,29 @@ class Engine(MinfftLibrary):
     def plan_bytes(self, aux: int) -> int:
         return int(self.lib.minfft_b200_plan_bytes(ctypes.c_void_p(aux)))
 
-    def plan_selfcheck(self, op: str, dims: Sequence[int], howmany: int = 1, alias: bool = False):
+    def plan_selfcheck(self, op: str, dims: Sequence[int], howmany: int = 1, alias: bool = False,
+                       precision: str = "fp32"):
         """Host-only planning check (no device): (violations, report, launch count)."""
         arr = (ctypes.c_int * len(dims))(*[int(d) for d in dims])
         buf = ctypes.create_string_buffer(4096)
         n = ctypes.c_int(0)
-        bad = self.lib.minfft_b200_plan_selfcheck(OP_CODES[op], len(dims), arr, int(howmany), int(alias), buf, 4096,
-                                                  ctypes.byref(n))
+        bad = self.lib.minfft_b200_plan_selfcheck_precision(OP_CODES[op], len(dims), arr, int(howmany), int(alias),
+                                                            PRECISIONS[precision], buf, 4096, ctypes.byref(n))
         return int(bad), buf.value.decode(), int(n.value)
+
+    def set_precision(self, aux: int, precision: str) -> None:
+        """Arithmetic of the plan's complex 256-point passes: "fp32", "tc_f16" or "tc_bf16"."""
+        if self.lib.minfft_b200_set_precision(ctypes.c_void_p(aux), PRECISIONS[precision]):
+            self.check()
+
+    def get_precision(self, aux: int) -> str:
+        code = int(self.lib.minfft_b200_get_precision(ctypes.c_void_p(aux)))
+        return {v: k for k, v in PRECISIONS.items()}[code]
+
+    def tc_status(self, aux: int) -> None:
+        """Raise if a tensor-core pass of the plan gave up waiting since the last call."""
+        if self.lib.minfft_b200_tc_status(ctypes.c_void_p(aux)):
+            self.check()
 
     def autotune(self, aux: int, op: str, howmany: int = 1, reps: int = 5) -> None:
         """Tune every launch of `op` on this plan (kernel form, tile size) on the device."""
@@ -295,5 +320,5 @@ def transform(op: str, x, dims: Optional[Sequence[int]] = None, single: Optional
     return out
 
 
-__all__ = ["ERROR_NAMES", "MixedJob", "Engine", "Plan", "MinfftError", "engine", "transform", "shapes", "OPS", "FAMILIES", "OP_FAMILY",
+__all__ = ["PRECISIONS", "ERROR_NAMES", "MixedJob", "Engine", "Plan", "MinfftError", "engine", "transform", "shapes", "OPS", "FAMILIES", "OP_FAMILY",
            "OP_CODES", "LIB_PATHS"]

@@ -36,6 +36,7 @@
 #include "kernel_registry.h"
 #include "pipe_pass.cuh"
 #include "line_kernels.h"
+#include "tc_pass.h"
 #include "minfft.h"
 #include "minfft_b200.h"
 
@@ -224,6 +225,8 @@ struct Launch {
   bool out_c = false;    // the kernel writes its output as complex values
   bool hbm_pass = false; // a pass of the Stockham FFT over HBM (never in place)
   bool pipe = false;     // persistent pipelined kernel (pipe_pass.cuh)
+  bool tc = false;       // tensor-core split-precision pass (tc_pass.cu)
+  mb::TcParams tcp{};    // its B operands and status word
   int ch_static = 16;    // pipelined kernel: copy chunk allowed by the strides
   int combo = -1;        // axis kernels: mb::Combo; line kernels: mb::LineKernel
   TuneKey key{};         // axis kernels: autotuning key
@@ -273,6 +276,8 @@ struct minfft_aux {
   void* bufs[BUF_COUNT] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   size_t buf_bytes[BUF_COUNT] = {0, 0, 0, 0, 0, 0};
   std::map<std::tuple<int, int, int>, Program> programs;  // (op, howmany, alias)
+  int precision = MINFFT_B200_PREC_FP32;  // arithmetic of the 256-point complex passes
+  void* tc_mem = nullptr;                 // tensor-core B operands (both formats) and status word
   void* stage_in = nullptr;
   size_t stage_in_bytes = 0;
   void* stage_out = nullptr;
@@ -456,11 +461,101 @@ struct Planner {
            sm <= (size_t)dev_max_smem;
   }
 
+  // The tensor-core pass covers complex 256-point axes without a
+  // pre-twiddle (every in-CTA axis of that length and the first pass of a
+  // Stockham chain); it always stages the tile through shared memory.
+  bool use_tc(int combo, int L, const AxisParams& ap) const {
+    return a->precision != MINFFT_B200_PREC_FP32 && combo == mb::K_CPLX && L == mb::kTcLength && ap.st_ns == 1 &&
+           (ap.flags & ~(mb::F_CONJ_IN | mb::F_CONJ_OUT | mb::F_STAGE_ROWS)) == 0;
+  }
+
+  void add_tc_kernel(int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, const TuneKey& key) {
+    const int fmt = a->precision == MINFFT_B200_PREC_TC_BF16 ? mb::TC_BF16 : mb::TC_F16;
+    const int tb = ap.colmode ? 16 : 8;  // column mode: 16 adjacent columns = 128-byte runs
+    Launch ln;
+    ln.key = key;
+    ln.radix = 16;
+    ln.tc = true;
+    ln.fn = mb::tc_kernel(fmt, tb);
+    if (!ln.fn) {
+      set_error(MINFFT_B200_EUNSUPPORTED, "the tensor-core pass needs the single-precision library");
+      ok = false;
+      return;
+    }
+    ln.smem = mb::tc_smem(fmt, tb);
+    if (ln.smem > (size_t)dev_max_smem) {
+      set_error(MINFFT_B200_EUNSUPPORTED, "shared memory %zu exceeds %d", ln.smem, dev_max_smem);
+      ok = false;
+      return;
+    }
+    if (!a->host_only && !ensure_smem_attr(ln.fn, ln.smem)) {
+      ok = false;
+      return;
+    }
+    if (a->host_only) {
+      static uint4 dummy[1];
+      ln.tcp.bmat = dummy;
+      ln.tcp.status = nullptr;
+    } else {
+      if (!a->tc_mem) {
+        set_error(MINFFT_B200_EINVAL, "tensor-core operands missing (set the precision first)");
+        ok = false;
+        return;
+      }
+      ln.tcp.bmat = static_cast<const char*>(a->tc_mem) + (fmt == mb::TC_F16 ? 0 : mb::tc_bmat_bytes(mb::TC_F16));
+      ln.tcp.status = reinterpret_cast<int*>(static_cast<char*>(a->tc_mem) + mb::tc_bmat_bytes(mb::TC_F16) +
+                                             mb::tc_bmat_bytes(mb::TC_BF16));
+    }
+    ap.cpb = tb;
+    ap.nbatch = nbatch;
+    ap.lp = 0;
+    ap.ntiles = (nbatch + tb - 1) / tb;
+    ln.block = unsigned(mb::tc_threads(tb));
+    // persistent: one CTA per resident slot.  The occupancy calculator
+    // reports one CTA per SM for kernels that allocate tensor memory, so the
+    // slots are counted here from registers, shared memory, threads and the
+    // 512 TMEM columns of an SM.
+    int occ = 1;
+    if (!a->host_only) {
+      cudaFuncAttributes fa;
+      int dev = 0, smem_sm = 0, regs_sm = 0;
+      if (cudaFuncGetAttributes(&fa, ln.fn) == cudaSuccess && cudaGetDevice(&dev) == cudaSuccess &&
+          cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+          cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) == cudaSuccess) {
+        const int warps = int(ln.block + 31) / 32;
+        const int regs_cta = warps * ((fa.numRegs * 32 + 255) / 256 * 256);
+        const size_t smem_cta = ln.smem + fa.sharedSizeBytes + 1024;  // + the per-CTA reservation
+        occ = std::min({regs_sm / std::max(regs_cta, 1), int(size_t(smem_sm) / smem_cta), 2048 / int(ln.block),
+                        512 / mb::tc_tmem_columns(tb)});
+        occ = std::max(occ, 1);
+      } else {
+        cudaGetLastError();
+      }
+    }
+    ln.grid = unsigned(std::min<int64_t>(ap.ntiles, int64_t(sms) * occ));
+    ln.in_buf = in_buf;
+    ln.out_buf = out_buf;
+    ln.in_c = ln.out_c = true;
+    ln.combo = mb::K_CPLX;
+    ln.L = L;
+    ln.ap = ap;
+    ln.bytes = 2.0 * L * sizeof(cpx) * double(nbatch);
+    char buf[160];
+    snprintf(buf, sizeof(buf), "tc_pass<%s,L=%d,%s> batch=%lld", fmt == mb::TC_F16 ? "f16x3" : "bf16x6", L,
+             ap.colmode ? "col" : "row", (long long)nbatch);
+    ln.label = buf;
+    prog->launches.push_back(ln);
+  }
+
   void add_axis_kernel(int combo, int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, bool vec_in,
                        bool vec_out) {
     const int lg = ilog2(L);
     const TuneKey key{combo, L, ap.colmode, ap.st_ns > 1 ? 1 : 0, (ap.flags & mb::F_STAGE_ROWS) ? 1 : 0,
                       nbatch, ap.d0, ap.in_n, ap.out_k};
+    if (use_tc(combo, L, ap)) {
+      add_tc_kernel(L, nbatch, ap, in_buf, out_buf, key);
+      return;
+    }
     TuneVal tv;
     int R = 16;  // per-thread radix of the one-tile-per-CTA form
     if (tune_lookup(key, &tv)) {
@@ -1111,6 +1206,11 @@ bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
     while (ch > 4 && (reinterpret_cast<uintptr_t>(ap.in) % ch) != 0) ch /= 2;
     ap.chunk = ch;
   }
+  if (ln.tc) {
+    mb::TcParams tcp = ln.tcp;
+    void* targs[2] = {&ap, &tcp};
+    return cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), targs, ln.smem, a->stream), "launch(tc)");
+  }
   args[0] = &ap;
   return cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, ln.smem, a->stream), "launch(axis)");
 }
@@ -1292,6 +1392,7 @@ MB_EXPORT void minfft_free_aux(minfft_aux* a) {
       if (a->bufs[b]) cudaFree(a->bufs[b]);
     if (a->stage_in) cudaFree(a->stage_in);
     if (a->stage_out) cudaFree(a->stage_out);
+    if (a->tc_mem) cudaFree(a->tc_mem);
     for (cudaEvent_t e : a->ev_pool) cudaEventDestroy(e);
   }
   delete a;
@@ -1386,6 +1487,63 @@ MB_EXPORT int minfft_b200_launch_count(int op, const minfft_aux* ca) {
   DeviceGuard guard(a->device);
   Program* p = get_program(a, op, 1, false);
   return p ? (int)p->launches.size() : -1;
+}
+
+MB_EXPORT int minfft_b200_set_precision(minfft_aux* a, int mode) {
+  if (!a || mode < MINFFT_B200_PREC_FP32 || mode > MINFFT_B200_PREC_TC_BF16) {
+    set_error(MINFFT_B200_EINVAL, "bad precision arguments");
+    return MINFFT_B200_EINVAL;
+  }
+  if (mode != MINFFT_B200_PREC_FP32 && sizeof(real) != 4) {
+    set_error(MINFFT_B200_EUNSUPPORTED, "tensor-core passes exist in the single-precision library only");
+    return MINFFT_B200_EUNSUPPORTED;
+  }
+  if (mode != MINFFT_B200_PREC_FP32 && !a->tc_mem) {
+    // both formats' B operands, then the status word
+    DeviceGuard guard(a->device);
+    const size_t b16 = mb::tc_bmat_bytes(mb::TC_F16), bb = mb::tc_bmat_bytes(mb::TC_BF16);
+    std::vector<uint16_t> img, img2;
+    mb::tc_bmat_host(mb::TC_F16, img);
+    mb::tc_bmat_host(mb::TC_BF16, img2);
+    img.insert(img.end(), img2.begin(), img2.end());
+    img.resize(img.size() + 8, 0);
+    void* d = nullptr;
+    if (!cuda_ok(cudaMalloc(&d, b16 + bb + 16), "cudaMalloc(tc operands)")) return g_err;
+    if (!cuda_ok(cudaMemcpy(d, img.data(), b16 + bb + 16, cudaMemcpyHostToDevice), "cudaMemcpy(tc operands)")) {
+      cudaFree(d);
+      return g_err;
+    }
+    a->tc_mem = d;
+    a->table_bytes += b16 + bb + 16;
+  }
+  if (a->precision != mode) {
+    a->precision = mode;
+    a->programs.clear();
+  }
+  return MINFFT_B200_OK;
+}
+
+MB_EXPORT int minfft_b200_get_precision(const minfft_aux* a) { return a ? a->precision : -1; }
+
+MB_EXPORT int minfft_b200_tc_status(const minfft_aux* ca) {
+  if (!ca) {
+    set_error(MINFFT_B200_EINVAL, "NULL plan");
+    return MINFFT_B200_EINVAL;
+  }
+  if (!ca->tc_mem) return MINFFT_B200_OK;
+  DeviceGuard guard(ca->device);
+  if (!cuda_ok(cudaStreamSynchronize(ca->stream), "cudaStreamSynchronize")) return g_err;
+  int* st = reinterpret_cast<int*>(static_cast<char*>(ca->tc_mem) + mb::tc_bmat_bytes(mb::TC_F16) +
+                                   mb::tc_bmat_bytes(mb::TC_BF16));
+  int v = 0;
+  if (!cuda_ok(cudaMemcpy(&v, st, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(tc status)")) return g_err;
+  if (v) {
+    const int zero = 0;
+    cudaMemcpy(st, &zero, sizeof(int), cudaMemcpyHostToDevice);
+    set_error(MINFFT_B200_ETIMEOUT, "a tensor-core pass gave up waiting for its matrix operations");
+    return MINFFT_B200_ETIMEOUT;
+  }
+  return MINFFT_B200_OK;
 }
 
 MB_EXPORT int minfft_b200_profile(minfft_aux* a, int enable) {
@@ -1499,11 +1657,13 @@ Extent launch_extent(const Launch& ln) {
 // user buffers, launch shapes, and no in-place use of the passes that
 // cannot run in place.  Returns the number of violations (0 = plan is
 // sound); a description of the first ones goes to `report`.
-MB_EXPORT int minfft_b200_plan_selfcheck(int op, int d, const int* Ns, int howmany, int alias, char* report,
-                                         int report_len, int* launches) {
+MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns, int howmany, int alias,
+                                                   int precision, char* report, int report_len, int* launches) {
   const int fam = op_family(op);
   std::string rep;
   if (fam < 0 || d < 1 || !Ns || howmany < 1) return -1;
+  if (precision < MINFFT_B200_PREC_FP32 || precision > MINFFT_B200_PREC_TC_BF16) return -1;
+  if (precision != MINFFT_B200_PREC_FP32 && sizeof(real) != 4) return -1;
   for (int i = 0; i < d; ++i)
     if (!is_pow2(Ns[i])) return -1;
   minfft_aux a;
@@ -1513,6 +1673,7 @@ MB_EXPORT int minfft_b200_plan_selfcheck(int op, int d, const int* Ns, int howma
   for (int i = 0; i < d; ++i) a.total *= Ns[i];
   a.device = -1;
   a.host_only = true;
+  a.precision = precision;
   Program prog;
   if (!build_program(&a, op, howmany, alias != 0, &prog)) {
     if (report && report_len > 0) snprintf(report, report_len, "planning failed: %s", g_msg);
@@ -1550,7 +1711,7 @@ MB_EXPORT int minfft_b200_plan_selfcheck(int op, int d, const int* Ns, int howma
                                                                  (ln.in_buf == BUF_Y && ln.out_buf == BUF_X)));
     if (alias_io && (ln.hbm_pass || (ln.is_line && ln.combo != mb::LK_UNIT)))
       fail("launch %zu (%s): runs in place but cannot", i, ln.label.c_str());
-    if (!ln.is_line && !ln.pipe && ln.grid > 0 && int64_t(ln.grid) * ln.ap.cpb < ln.ap.nbatch)
+    if (!ln.is_line && !ln.pipe && !ln.tc && ln.grid > 0 && int64_t(ln.grid) * ln.ap.cpb < ln.ap.nbatch)
       fail("launch %zu: grid does not cover the batch", i);
     if (ln.pipe) {
       const AxisParams& ap = ln.ap;
@@ -1571,10 +1732,23 @@ MB_EXPORT int minfft_b200_plan_selfcheck(int op, int d, const int* Ns, int howma
               size_t(ap.cpb) * mb::tile_pitch(ln.L, std::min(ln.radix, ln.L), ap.cpb, ap.colmode) * sizeof(cpx))
         fail("launch %zu: stage of %d bytes too small", i, ap.stage_bytes);
     }
+    if (ln.tc) {
+      if (ln.L != mb::kTcLength || ln.combo != mb::K_CPLX || ln.ap.st_ns != 1)
+        fail("launch %zu (%s): tensor-core pass on an unsupported axis", i, ln.label.c_str());
+      if (ln.ap.cpb != 8 && ln.ap.cpb != 16) fail("launch %zu: tensor-core tile of %d transforms", i, ln.ap.cpb);
+      if (ln.ap.ntiles * ln.ap.cpb < ln.ap.nbatch || ln.grid < 1 || int64_t(ln.grid) > ln.ap.ntiles)
+        fail("launch %zu: tensor-core tiles do not cover the batch", i);
+    }
   }
   if (launches) *launches = (int)prog.launches.size();
   if (report && report_len > 0) snprintf(report, report_len, "%s", rep.c_str());
   return bad;
+}
+
+MB_EXPORT int minfft_b200_plan_selfcheck(int op, int d, const int* Ns, int howmany, int alias, char* report,
+                                         int report_len, int* launches) {
+  return minfft_b200_plan_selfcheck_precision(op, d, Ns, howmany, alias, MINFFT_B200_PREC_FP32, report, report_len,
+                                              launches);
 }
 
 // ------------------------------------------------------------- autotuner
@@ -1621,7 +1795,7 @@ MB_EXPORT int minfft_b200_autotune(minfft_aux* a, int op, int howmany, int reps)
   if (!p0) return g_err ? g_err : MINFFT_B200_ECUDA;
   std::vector<TuneKey> keys;
   for (const Launch& ln : p0->launches)
-    if (!ln.is_line) keys.push_back(ln.key);
+    if (!ln.is_line && !ln.tc) keys.push_back(ln.key);
   const size_t in_b = size_t(io_bytes(a, op, false)) * howmany, out_b = size_t(io_bytes(a, op, true)) * howmany;
   void *x = nullptr, *y = nullptr;
   if (!cuda_ok(cudaMalloc(&x, in_b), "cudaMalloc(autotune)")) return g_err;

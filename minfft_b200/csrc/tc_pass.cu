@@ -1,0 +1,474 @@
+// Tensor-core split-precision axis pass (single-precision library).
+//
+// A batch of complex DFTs of length 256 = 16 x 16 along one axis, computed as
+// two radix-16 stages, each a dense 16-point DFT-matrix contraction on the
+// 5th-generation tensor cores:
+//
+//   stage 1: for every transform t and low digit n2, the 16 values
+//            x[16*n1 + n2] (n1 = 0..15) are transformed over n1 and result
+//            k1 is multiplied by w_256^(n2*k1);
+//   stage 2: for every t and k1 the 16 values of stage 1 (n2 = 0..15) are
+//            transformed over n2, giving output k1 + 16*k2.
+//
+// One thread per sub-DFT: a CTA of 16*TB threads holds TB transforms, i.e.
+// 16*TB sub-DFTs per stage, in TB/8 groups of 128 rows (one UMMA of M = 128
+// per group).  A 16-point complex DFT is the real 32 x 32 matrix
+// [[C, S], [-S, C]] (C = cos, S = sin of 2*pi*k*n/16) acting on
+// (Re x, Im x), so a stage is D[128 x 32] = A[128 x 32] * B^T with A the
+// sub-DFT inputs (K-major, one row per sub-DFT) and B the fixed matrix.
+// Tensor cores take FP16 or BF16 operands; to keep FP32 accuracy every row
+// of A is scaled by its own power of two (bringing its largest component to
+// [256, 512)) and split into 16-bit terms, as is B:
+//   FP16: A = A0 + A1, B = B0 + B1 (11 + 11 significant bits), D = A0 B0 +
+//         A0 B1 + A1 B0                                  (3 products)
+//   BF16: A = A0 + A1 + A2 (8 + 8 + 8 bits), likewise B; the six products
+//         Ai Bj with i + j <= 2 are kept.
+// Products accumulate in FP32 in tensor memory and are read back with
+// tcgen05.ld.  The leading product A0 B0 and the correction products go to
+// two separate accumulators (32 columns each per group) that are added on the
+// CUDA cores: the matrix units round each accumulation step, and keeping the
+// long chain of small corrections away from the leading sum leaves only the
+// two K steps of A0 B0 to round at full magnitude.  The unscaling and the
+// twiddles between the stages also run on the CUDA cores.
+//
+// Synchronisation: warp 0 allocates and frees the TMEM columns; thread 0
+// issues the MMAs and commits them to an mbarrier; every thread waits on it
+// with a bounded spin.  A wait that runs out records the failure in
+// *status, the CTA skips its remaining work, waits once more (bounded) for
+// the MMAs in flight, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "axis_pass.cuh"
+#include "tc_pass.h"
+
+namespace mb {
+
+// ------------------------------------------------------------ host side
+void tc_split_host(int fmt, float v, uint16_t* terms) {
+  float r = v;
+  for (int i = 0; i < tc_terms(fmt); ++i) {
+    if (fmt == TC_F16) {
+      const __half h = __float2half_rn(r);
+      terms[i] = __half_as_ushort(h);
+      r -= __half2float(h);
+    } else {
+      const __nv_bfloat16 h = __float2bfloat16_rn(r);
+      terms[i] = __bfloat16_as_ushort(h);
+      r -= __bfloat162float(h);
+    }
+  }
+}
+
+void tc_bmat_host(int fmt, std::vector<uint16_t>& out) {
+  const int nt = tc_terms(fmt);
+  out.assign(size_t(nt) * 32 * 32, 0);
+  // cos and sin of 2*pi*m/16, zeros exact
+  double c16[16], s16[16];
+  for (int m = 0; m < 16; ++m) {
+    const double a = 2.0 * 3.141592653589793238462643383279502884 * m / 16.0;
+    c16[m] = (m % 8 == 4) ? 0.0 : std::cos(a);
+    s16[m] = (m % 8 == 0) ? 0.0 : std::sin(a);
+  }
+  for (int n = 0; n < 32; ++n)
+    for (int k = 0; k < 32; ++k) {
+      const int m = ((n & 15) * (k & 15)) & 15;
+      double v;
+      if (n < 16)
+        v = k < 16 ? c16[m] : s16[m];
+      else
+        v = k < 16 ? -s16[m] : c16[m];
+      uint16_t t[3];
+      tc_split_host(fmt, float(v), t);
+      for (int s = 0; s < nt; ++s) out[size_t(s) * 1024 + tc_operand_offset(n, k) / 2] = t[s];
+    }
+}
+
+#if MINFFT_SINGLE
+
+namespace {
+
+constexpr int kL = kTcLength;
+constexpr int kLP = 273;  // tile pitch in complex values: odd, so adjacent columns fall in distinct banks
+constexpr int kOpBytes = 128 * 32 * 2;  // A operand of one group: 128 rows x 32 columns x 16 bits
+constexpr int kBBytes = 32 * 32 * 2;    // B operand: 32 rows x 32 columns
+constexpr long long kSpinLimit = 1LL << 20;
+
+template <int FMT, int TB>
+struct TcLayout {
+  static constexpr int G = TB / 8;
+  static constexpr int NT = FMT == TC_F16 ? 2 : 3;
+  // A operands (written after the tile has been read into registers) and
+  // the data tile share one region
+  static constexpr int a_bytes = NT * G * kOpBytes;
+  static constexpr int d_bytes = (TB * kLP * int(sizeof(cpx)) + 15) / 16 * 16;
+  static constexpr int region = a_bytes > d_bytes ? a_bytes : d_bytes;
+  static constexpr int b_off = region;
+  static constexpr int offs_off = b_off + NT * kBBytes;
+  static constexpr int mbar_off = offs_off + 4 * TB * 8;  // two sets of tile offsets
+  static constexpr int total = mbar_off + 16;
+  static constexpr int tmem_cols = 64 * G;  // per group: leading accumulator, correction accumulator
+  static_assert(tmem_cols == 64 * (TB / 8), "tc_tmem_columns");
+};
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+  // start address >> 4; leading byte offset (between the two 8-column
+  // blocks of one K step) 128 B; stride byte offset (between 8-row blocks)
+  // 512 B; descriptor version 1; base offset 0; no swizzle
+  return uint64_t((saddr >> 4) & 0x3FFF) | (uint64_t(128 >> 4) << 16) | (uint64_t(512 >> 4) << 32) | (1ull << 46);
+}
+
+template <int FMT>
+__device__ __forceinline__ constexpr uint32_t instr_desc() {
+  // D format F32 (bits 4-5), A and B formats (7-9, 10-12: 0 FP16, 1 BF16),
+  // both K-major (15, 16 zero), N >> 3 (17-22), M >> 4 (24-28)
+  return (1u << 4) | (uint32_t(FMT) << 7) | (uint32_t(FMT) << 10) | (uint32_t(32 >> 3) << 17) |
+         (uint32_t(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t"
+      "}\n" ::"r"(dtmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+// Splits the pair (a, b) into NT packed 16-bit pairs (a in the low half),
+// each the correctly rounded value of the remainder: one packed conversion
+// per term, the remainders formed exactly in FP32.
+template <int FMT, int NT>
+__device__ __forceinline__ void split_pair(float a, float b, uint32_t (&w)[3]) {
+#pragma unroll
+  for (int i = 0; i < NT; ++i) {
+    if (FMT == TC_F16) {
+      const __half2 h = __floats2half2_rn(a, b);
+      w[i] = *reinterpret_cast<const uint32_t*>(&h);
+      if (i + 1 < NT) {
+        const float2 f = __half22float2(h);
+        a -= f.x;
+        b -= f.y;
+      }
+    } else {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+      w[i] = *reinterpret_cast<const uint32_t*>(&h);
+      if (i + 1 < NT) {
+        a -= __uint_as_float(w[i] << 16);
+        b -= __uint_as_float(w[i] & 0xFFFF0000u);
+      }
+    }
+  }
+}
+
+// 16 consecutive FP32 columns of this warp's 32 TMEM lanes
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&d)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), "=r"(d[8]),
+        "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
+      : "r"(taddr)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+  for (long long i = 0; i < kSpinLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t"
+        "}"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 2^s for integer s in [-126, 127]
+__device__ __forceinline__ float pow2i(int s) { return __int_as_float((127 + s) << 23); }
+
+// The 16 input values this thread moves of tile `tile` (element e = tid +
+// i * 16*TB of the tile's TB x 256 values; zero beyond the batch).
+template <int TB>
+__device__ __forceinline__ void load_tile(const AxisParams& p, const int64_t* offs, int nv, int tid, cpx (&v)[16]) {
+  const cpx* in = static_cast<const cpx*>(p.in);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int e = tid + i * 16 * TB;
+    const int c = p.colmode ? (e % TB) : (e / kL);
+    const int n = p.colmode ? (e / TB) : (e % kL);
+    v[i] = c < nv ? in[offs[c] + int64_t(n) * p.in_n] : czero();
+  }
+}
+
+// Offsets of the TB transforms of tile `tile` (threads 0..TB-1).
+template <int TB>
+__device__ __forceinline__ void tile_offsets(const AxisParams& p, int64_t tile, int tid, int64_t* offs) {
+  if (tid < TB) {
+    const int64_t b = tile * TB + tid;
+    int64_t b0, oi, oo;
+    batch_offsets(p, b < p.nbatch ? b : 0, b0, oi, oo);
+    offs[tid] = oi;
+    offs[TB + tid] = oo;
+  }
+}
+
+// Persistent: CTA k handles tiles k, k + gridDim.x, ...; while the tensor
+// cores work on one tile, the next tile's inputs are already on their way
+// into registers.
+template <int FMT, int TB>
+__global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const AxisParams p, const TcParams q) {
+  using Lay = TcLayout<FMT, TB>;
+  constexpr int G = Lay::G, NT = Lay::NT, NTHR = 16 * TB;
+  extern __shared__ __align__(128) unsigned char sm[];
+  unsigned char* aop = sm;
+  cpx* data = reinterpret_cast<cpx*>(sm);
+  unsigned char* bop = sm + Lay::b_off;
+  int64_t* offs = reinterpret_cast<int64_t*>(sm + Lay::offs_off);  // two sets of 2*TB (tile parity)
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + Lay::mbar_off);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + Lay::mbar_off + 8);
+  int* bad = reinterpret_cast<int*>(sm + Lay::mbar_off + 12);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const uint32_t mbar_a = static_cast<uint32_t>(__cvta_generic_to_shared(mbar));
+  const int64_t ntiles = (p.nbatch + TB - 1) / TB;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(tslot))),
+                 "n"(Lay::tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *bad = 0;
+  }
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(q.bmat);
+    uint4* dst = reinterpret_cast<uint4*>(bop);
+    for (int i = tid; i < NT * kBBytes / 16; i += NTHR) dst[i] = src[i];
+  }
+  int64_t tile = blockIdx.x;
+  tile_offsets<TB>(p, tile, tid, offs);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  const bool cj_in = (p.flags & F_CONJ_IN) != 0, cj_out = (p.flags & F_CONJ_OUT) != 0;
+  constexpr uint32_t idesc = instr_desc<FMT>();
+  const uint32_t aop_a = static_cast<uint32_t>(__cvta_generic_to_shared(aop));
+  const uint32_t bop_a = static_cast<uint32_t>(__cvta_generic_to_shared(bop));
+  const int grp = tid >> 7, row = tid & 127;  // UMMA group and row of this thread's sub-DFT
+  const int t = tid >> 4, dgt = tid & 15;     // its transform and digit
+  bool ok = true;
+  uint32_t phase = 0;
+
+  cpx v[16];
+  auto valid = [&](int64_t tl) {
+    const int64_t left = p.nbatch - tl * TB;
+    return int(left < TB ? left : TB);
+  };
+  if (tile < ntiles) load_tile<TB>(p, offs, valid(tile), tid, v);
+
+#pragma unroll 1
+  for (int par = 0; tile < ntiles && ok; tile += gridDim.x, par ^= 1) {
+    const int64_t* cur = offs + par * 2 * TB;
+    // ---- the tile's inputs into shared memory (the previous tile's store
+    // has finished reading it)
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int e = tid + i * NTHR;
+      const int c = p.colmode ? (e % TB) : (e / kL);
+      const int n = p.colmode ? (e / TB) : (e % kL);
+      cpx x = v[i];
+      if (cj_in) x.y = -x.y;
+      data[c * kLP + pad16(n)] = x;
+    }
+    const int64_t next = tile + gridDim.x;
+    int64_t* nxt = offs + (par ^ 1) * 2 * TB;
+    if (next < ntiles) tile_offsets<TB>(p, next, tid, nxt);
+    __syncthreads();
+    // ---- the next tile's loads are issued now and land during the stages
+    if (next < ntiles) load_tile<TB>(p, nxt, valid(next), tid, v);
+
+#pragma unroll 1
+    for (int stage = 0; stage < 2; ++stage) {
+      // ---- this row's inputs: stage 1 x[16*n1 + n2], stage 2 y[16*k1 + n2]
+      float re[16], im[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int pos = stage == 0 ? 16 * i + dgt : 16 * dgt + i;
+        const cpx u = data[t * kLP + pad16(pos)];
+        re[i] = u.x;
+        im[i] = u.y;
+      }
+      float mx = 0.f;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) mx = fmaxf(mx, fmaxf(fabsf(re[i]), fabsf(im[i])));
+      // row scale 2^s with the largest component scaled into [2^8, 2^9)
+      const int ex = (__float_as_int(mx) >> 23) & 0xFF;  // biased exponent (mx >= 0)
+      const int s = min(max(135 - ex, -126), 126);
+      const float sc = pow2i(s), inv = pow2i(-s);
+      __syncthreads();  // the tile is read: the A operands overwrite it
+      // ---- split into NT terms and write the A operands (K: Re 0..15, Im 16..31)
+#pragma unroll
+      for (int kb = 0; kb < 4; ++kb) {
+        uint32_t w[NT][4];
+#pragma unroll
+        for (int u = 0; u < 8; u += 2) {
+          uint32_t o[3];
+          const int k = kb * 8 + u;
+          split_pair<FMT, NT>((k < 16 ? re[k] : im[k - 16]) * sc, (k + 1 < 16 ? re[k + 1] : im[k + 1 - 16]) * sc, o);
+#pragma unroll
+          for (int z = 0; z < NT; ++z) w[z][u / 2] = o[z];
+        }
+#pragma unroll
+        for (int z = 0; z < NT; ++z)
+          *reinterpret_cast<uint4*>(aop + (z * G + grp) * kOpBytes + tc_operand_offset(row, kb * 8)) =
+              make_uint4(w[z][0], w[z][1], w[z][2], w[z][3]);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      // ---- the MMAs, two K steps of 16 each: per group, the corrections
+      // Ai Bj (0 < i + j < NT, smallest first) into columns 64g+32.., then
+      // the leading A0 B0 into columns 64g..
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          uint32_t acc = 0;
+#pragma unroll
+          for (int sum = NT - 1; sum >= 1; --sum)
+#pragma unroll
+            for (int i = 0; i <= sum; ++i) {
+              const int j = sum - i;
+#pragma unroll
+              for (int kh = 0; kh < 2; ++kh) {
+                const uint64_t ad = smem_desc(aop_a + (i * G + g) * kOpBytes + kh * 256);
+                const uint64_t bd = smem_desc(bop_a + j * kBBytes + kh * 256);
+                mma_f16(tmem + uint32_t(64 * g + 32), ad, bd, idesc, acc);
+                acc = 1;
+              }
+            }
+#pragma unroll
+          for (int kh = 0; kh < 2; ++kh) {
+            const uint64_t ad = smem_desc(aop_a + g * kOpBytes + kh * 256);
+            const uint64_t bd = smem_desc(bop_a + kh * 256);
+            mma_f16(tmem + uint32_t(64 * g), ad, bd, idesc, kh);
+          }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_a)
+                     : "memory");
+      }
+      if (!mbar_wait(mbar_a, phase)) atomicExch(bad, 1);
+      __syncthreads();
+      if (*bad) {
+        ok = false;
+        break;
+      }
+      phase ^= 1;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // ---- this row of D: columns 0..15 Re y_k, 16..31 Im y_k of both
+      // accumulators (TMEM lanes 32*(warp % 4) .. +31)
+      const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(64 * grp);
+      {
+        uint32_t d[16], e[16];
+        tmem_ld16(taddr, d);
+        tmem_ld16(taddr + 32, e);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int k = 0; k < 16; ++k) re[k] = (__uint_as_float(d[k]) + __uint_as_float(e[k])) * inv;
+        tmem_ld16(taddr + 16, d);
+        tmem_ld16(taddr + 48, e);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int k = 0; k < 16; ++k) im[k] = (__uint_as_float(d[k]) + __uint_as_float(e[k])) * inv;
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      // the MMAs have completed (mbarrier), so the A region is free again
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        cpx y = cmk(re[k], im[k]);
+        if (stage == 0) {
+          y = cmul(y, ldg(p.tw + dgt * k));  // w_256^(n2*k1): n2 = digit, k1 = k
+          data[t * kLP + pad16(16 * k + dgt)] = y;
+        } else {
+          data[t * kLP + pad16(dgt + 16 * k)] = y;  // output k1 + 16*k2 with k1 = digit, k2 = k
+        }
+      }
+      __syncthreads();
+    }
+    if (!ok) break;
+
+    // ---- store the tile
+    {
+      cpx* out = static_cast<cpx*>(p.out);
+      const int nv = valid(tile);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int e = tid + i * NTHR;
+        const int c = p.colmode ? (e % TB) : (e / kL);
+        const int n = p.colmode ? (e / TB) : (e % kL);
+        if (c < nv) {
+          cpx x = data[c * kLP + pad16(n)];
+          if (cj_out) x.y = -x.y;
+          out[cur[TB + c] + int64_t(n) * p.out_k] = x;
+        }
+      }
+    }
+    __syncthreads();  // the tile is stored: the next one may overwrite it
+  }
+
+  if (!ok) {
+    if (tid == 0 && q.status) atomicExch(q.status, 1);
+    // the MMAs of the abandoned stage may still be running: give them one
+    // more bounded wait before the columns are released
+    mbar_wait(mbar_a, phase);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(Lay::tmem_cols)
+                 : "memory");
+  }
+}
+
+}  // namespace
+
+const void* tc_kernel(int fmt, int tb) {
+  if (fmt == TC_F16) {
+    if (tb == 8) return (const void*)tc256_kernel<TC_F16, 8>;
+    if (tb == 16) return (const void*)tc256_kernel<TC_F16, 16>;
+  } else if (fmt == TC_BF16) {
+    if (tb == 8) return (const void*)tc256_kernel<TC_BF16, 8>;
+    if (tb == 16) return (const void*)tc256_kernel<TC_BF16, 16>;
+  }
+  return nullptr;
+}
+
+size_t tc_smem(int fmt, int tb) {
+  if (fmt == TC_F16) return tb == 8 ? TcLayout<TC_F16, 8>::total : TcLayout<TC_F16, 16>::total;
+  return tb == 8 ? TcLayout<TC_BF16, 8>::total : TcLayout<TC_BF16, 16>::total;
+}
+
+#else
+
+const void* tc_kernel(int, int) { return nullptr; }
+size_t tc_smem(int, int) { return 0; }
+
+#endif
+
+}  // namespace mb

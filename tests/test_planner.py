@@ -78,3 +78,27 @@ def test_every_launch_configuration_is_in_bounds(single, pipe, radix):
                         assert bad == 0, f"pipe={pipe} cpb={cpb} {op} {dims} alias={alias}:\n{rep}"
     finally:
         eng.tune_set_default(-1, 0)
+
+
+TC_SHAPES = [(256,), (4, 256), (256, 2), (256, 256), (256, 256, 256), (64, 64, 256), (256, 16, 4), (65536, 2),
+             (1 << 16,), (1 << 24,), (2, 256, 2)]
+
+
+@pytest.mark.parametrize("precision", ["tc_f16", "tc_bf16"])
+@pytest.mark.parametrize("dims", TC_SHAPES, ids=lambda d: "x".join(map(str, d)))
+def test_tensor_core_plans_are_in_bounds(dims, precision):
+    """The tensor-core passes replace every complex 256-point axis pass without
+    a pre-twiddle; the plans stay sound and keep their launch counts."""
+    eng = minfft_b200.engine(True)
+    for op in OPS:
+        for howmany, alias in itertools.product((1, 3), (False, True)):
+            bad, rep, n = eng.plan_selfcheck(op, dims, howmany, alias, precision=precision)
+            assert bad == 0, f"{op} {dims} {precision} howmany={howmany} alias={alias}:\n{rep}"
+            _, _, n32 = eng.plan_selfcheck(op, dims, howmany, alias)
+            assert n == n32
+
+
+def test_tensor_core_modes_need_the_single_library():
+    eng = minfft_b200.engine(False)
+    bad, _, _ = eng.plan_selfcheck("dft", (256,), 1, False, precision="tc_f16")
+    assert bad == -1

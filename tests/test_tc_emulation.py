@@ -1,0 +1,94 @@
+"""CPU model of the tensor-core split-precision arithmetic (the scheme the
+kernel in minfft_b200/csrc/tc_pass.cu runs on tcgen05), checked against the
+double-precision oracle.
+
+Per radix-16 stage, each row of 16 complex inputs is scaled by a power of two
+so that its largest component lies in [256, 512), split into 16-bit terms
+(FP16: two, BF16: three) and multiplied by the split real 32 x 32 form of the
+16-point DFT matrix, keeping the products Ai Bj with i + j < terms and
+accumulating in FP32; the result is unscaled and twiddled in FP32.  The model
+shows the scheme itself meets the 1e-6 relative-L2 bar with margin, so the GPU
+tests measure the kernel, not the method."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import rel_l2
+
+F32 = np.float32
+
+
+def to16(r, fmt):
+    """Round FP32 values to FP16 or BF16 (nearest even), returned as FP32."""
+    if fmt == "f16":
+        return r.astype(np.float16).astype(F32)
+    b = r.astype(F32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) >> 16 << 16
+    return b.astype(np.uint32).view(F32)
+
+
+def split(v, fmt):
+    terms, r = [], v.astype(F32)
+    for _ in range(2 if fmt == "f16" else 3):
+        h = to16(r, fmt)
+        terms.append(h)
+        r = (r - h).astype(F32)
+    return terms
+
+
+def dft16_real():
+    m = (np.arange(16)[:, None] * np.arange(16)[None, :]) % 16
+    c = np.cos(2 * np.pi * m / 16)
+    s = np.sin(2 * np.pi * m / 16)
+    c[m % 8 == 4] = 0
+    s[m % 8 == 0] = 0
+    return np.block([[c, s], [-s, c]]).astype(F32)
+
+
+def stage(rows, fmt):
+    a = np.concatenate([rows.real, rows.imag], axis=1).astype(F32)
+    mx = np.abs(a).max(axis=1)
+    ex = ((mx.view(np.uint32) >> 23) & 0xFF).astype(np.int64)
+    sc = np.ldexp(np.ones_like(mx), np.clip(135 - ex, -126, 126)).astype(F32)
+    at, bt = split(a * sc[:, None], fmt), split(dft16_real(), fmt)
+    d = np.zeros((a.shape[0], 32), F32)
+    for i in range(len(at)):
+        for j in range(len(at) - i):
+            d = (d + (at[i].astype(np.float64) @ bt[j].T.astype(np.float64)).astype(F32)).astype(F32)
+    d = (d / sc[:, None]).astype(F32)
+    return (d[:, :16] + 1j * d[:, 16:]).astype(np.complex64)
+
+
+def tc256(x, fmt):
+    t = x.shape[0]
+    v = x.astype(np.complex64).reshape(t, 16, 16)                  # [t, n1, n2]
+    y = stage(v.transpose(0, 2, 1).reshape(t * 16, 16), fmt).reshape(t, 16, 16)  # [t, n2, k1]
+    tw = np.exp(-2j * np.pi * np.outer(np.arange(16), np.arange(16)) / 256).astype(np.complex64)
+    y = (y * tw[None]).astype(np.complex64)
+    z = stage(y.transpose(0, 2, 1).reshape(t * 16, 16), fmt).reshape(t, 16, 16)  # [t, k1, k2]
+    return z.transpose(0, 2, 1).reshape(t, 256)
+
+
+@pytest.mark.parametrize("fmt", ["f16", "bf16"])
+@pytest.mark.parametrize("spread", [0.0, 20.0])
+def test_split_scheme_meets_the_bar(fmt, spread):
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((64, 256)) + 1j * rng.standard_normal((64, 256))
+    x *= np.exp(rng.uniform(-spread, spread, (64, 1)))
+    got = tc256(x, fmt)
+    for i in range(x.shape[0]):
+        ref = oracle.apply("dft", x[i].astype(np.complex128), (256,), single=False, kind=oracle.best_kind())
+        assert rel_l2(got[i], ref) <= 3e-7, (fmt, i)
+
+
+def test_split_terms_reconstruct_fp32():
+    """Rows scaled into [256, 512): FP16 pairs keep 2^-22 of the row maximum
+    (FP16's subnormal floor bounds the small elements), BF16 triples keep
+    every element to 2^-23 of itself."""
+    rng = np.random.default_rng(6)
+    v = (rng.standard_normal(10000) * 100).astype(F32)
+    v = np.clip(v, -511, 511).astype(F32)
+    s = sum(t.astype(np.float64) for t in split(v, "f16"))
+    assert np.max(np.abs(s - v)) <= 2.0 ** -22 * 256
+    s = sum(t.astype(np.float64) for t in split(v, "bf16"))
+    assert np.max(np.abs(s - v) / np.abs(v)) <= 2.0 ** -23
