@@ -66,22 +66,56 @@ def peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while running."""
+    """Samples SM clocks and clock-event (throttle) reasons while running:
+    through NVML every 10 ms (read-only queries), else nvidia-smi every 100 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.stop = threading.Event()
+        self.samples = []  # (sm_mhz, max_mhz, set of reason names)
+        self.source = None
 
     def __enter__(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                        rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((float(sm), float(mx), {n for n, b in bits.items() if rs & b}))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.01)
+
+            self.nvml = pynvml
+            self.source = "nvml 10 ms"
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi 100 ms"
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
@@ -89,10 +123,20 @@ class ClockSampler:
         return self
 
     def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        for ln in self.proc.stdout:
+            parts = [p.strip() for p in ln.strip().split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                self.samples.append((float(parts[1]), float(parts[2]),
+                                     {nm for nm, v in zip(self.NAMES, parts[5:9]) if v.lower() == "active"}))
+            except ValueError:
+                continue
 
     def __exit__(self, *exc):
+        self.stop.set()
+        if self.nvml is not None:
+            self.thread.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -101,22 +145,13 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
+        sm = [a for a, _, _ in self.samples]
+        mx = self.samples[-1][1] if self.samples else None
+        reasons = set()
+        for _, _, r in self.samples:
+            reasons |= r
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": self.source}
 
 
 # ---------------------------------------------------------------- workloads
@@ -366,7 +401,7 @@ class WorkloadMixed:
 
     @staticmethod
     def cpu_sample(P):
-        return f"the whole 20000-transform batch once, each (kind, n) group as an OpenMP batch on {P} threads"
+        return f"the whole 20000-transform batch, each (kind, n) group as an OpenMP batch on {P} threads"
 
     def tune(self):
         self.eng.mixed_autotune(self.handle, 3)
@@ -380,6 +415,10 @@ class WorkloadMixed:
 
     def launches_per_step(self):
         return 1
+
+    def roofline_stats(self, ms, steps):
+        """One graph launch of the persistent kernel per step: its time is the step time."""
+        return [("f32 mixed_kernel (graph launch)", steps, ms, float(self.in_bytes + self.out_bytes))]
 
     def e2e_setup(self):
         t = self.torch
@@ -407,7 +446,205 @@ class WorkloadMixed:
     cpu_sequences = ()
 
 
-WORKLOADS = {"2d2048": Workload2D, "batch4096": WorkloadBatch4096, "mixed20000": WorkloadMixed}
+class Workload3D256:
+    """256 x 256 x 256 complex DFT, forward then inverse, c64.  The arithmetic
+    of its 256-point axis passes follows --precision: "fp32" (CUDA cores) or
+    the tensor-core split-precision passes "tc_f16" / "tc_bf16"."""
+
+    name = "3d256"
+    dims = (256, 256, 256)
+    nsets = 3
+    dtype = "f32"
+    precision = "fp32"
+
+    def __init__(self, torch, dev):
+        import minfft_b200
+
+        self.torch = torch
+        n = int(np.prod(self.dims))
+        self.flops_per_transform = 5.0 * n * math.log2(n)
+        self.ops_per_step = 2
+        self.eng = minfft_b200.engine(True)
+        rng = np.random.default_rng(3)
+        mk = lambda: torch.from_numpy((rng.standard_normal(self.dims) + 1j * rng.standard_normal(self.dims))  # noqa
+                                      .astype(np.complex64)).to(dev)
+        self.xs = [mk() for _ in range(self.nsets)]
+        self.y = torch.empty(self.dims, dtype=torch.complex64, device=dev)
+        self.z = torch.empty(self.dims, dtype=torch.complex64, device=dev)
+        self.plan = self._mkplan()
+        # accuracy of this precision against the double-precision engine on the same input
+        e64 = minfft_b200.engine(False)
+        p64 = e64.plan("dft", self.dims)
+        x64 = self.xs[0].to(torch.complex128)
+        y64 = torch.empty_like(x64)
+        p64("dft", x64.data_ptr(), y64.data_ptr())
+        self.plan("dft", self.xs[0].data_ptr(), self.y.data_ptr())
+        self.plan("invdft", self.y.data_ptr(), self.z.data_ptr())
+        torch.cuda.synchronize()
+        self.eng.tc_status(self.plan.aux)
+        self.err = float(torch.linalg.vector_norm(self.y.to(torch.complex128) - y64) / torch.linalg.vector_norm(y64))
+        self.roundtrip = float(torch.linalg.vector_norm(self.z.to(torch.complex128) / n - x64) /
+                               torch.linalg.vector_norm(x64))
+        p64.free()
+        del x64, y64
+
+    def _mkplan(self):
+        plan = self.eng.plan("dft", self.dims)
+        self.eng.set_precision(plan.aux, self.precision)
+        return plan
+
+    def plans(self):
+        yield self.eng, self.plan, ("dft", "invdft")
+
+    def rebuild(self, eng, plan):
+        self.plan.free()
+        self.plan = self._mkplan()
+
+    def step(self, k):
+        x = self.xs[k % self.nsets]
+        self.plan("dft", x.data_ptr(), self.y.data_ptr(), check=False)
+        self.plan("invdft", self.y.data_ptr(), self.z.data_ptr(), check=False)
+
+    def check_errors(self):
+        self.eng.check()
+        self.eng.tc_status(self.plan.aux)
+
+    def launches_per_step(self):
+        return sum(self.eng.launch_count(op, self.plan.aux) for op in ("dft", "invdft"))
+
+    def e2e_setup(self):
+        t = self.torch
+        self.hx = t.empty(self.dims, dtype=t.complex64, pin_memory=True)
+        self.hx.copy_(self.xs[0].cpu())
+        self.hy = t.empty_like(self.hx, pin_memory=True)
+        self.hz = t.empty_like(self.hx, pin_memory=True)
+        b = self.hx.numel() * 8
+        return 2 * b, 2 * b
+
+    def e2e_step(self):
+        self.plan("dft", self.hx.data_ptr(), self.hy.data_ptr(), check=False)
+        self.plan("invdft", self.hy.data_ptr(), self.hz.data_ptr(), check=False)
+
+    def config(self):
+        return {"workload": "3-D complex DFT 256x256x256 c64, forward then inverse", "dims": list(self.dims),
+                "precision": self.precision,
+                "rel_l2_vs_f64_engine": self.err, "roundtrip_rel_l2": self.roundtrip,
+                "flops": "5*N*log2(N) per transform, N=2^24",
+                "inputs": "re/im i.i.d. standard normal, numpy PCG64 seed 3",
+                "l2": "inputs rotate over 3 sets of 128 MiB, larger than the 126 MB L2"}
+
+    cpu_sequences = (("dft", ("dft", "invdft"), True),)
+
+    @classmethod
+    def cpu_measure(cls, kind, threads, warm, reps):
+        t = cpu_run(kind, cls.cpu_sequences, cls.dims, threads, threads, reps, warm)
+        n = int(np.prod(cls.dims))
+        return t, 5.0 * n * math.log2(n) * 2 * threads * reps
+
+
+class WorkloadLong1D:
+    """Long 1-D transforms: complex DFT of 2^26 points in c128 and c64, and
+    DCT-4 + DST-4 of 2^24 points in f64 and f32."""
+
+    name = "long1d"
+    n_dft, n_t4 = 1 << 26, 1 << 24
+    nsets = 2
+    dtype = "f64+f32"
+
+    def __init__(self, torch, dev):
+        import minfft_b200
+
+        self.torch = torch
+        fd = 5.0 * self.n_dft * math.log2(self.n_dft)
+        f4 = 2.5 * self.n_t4 * math.log2(self.n_t4)
+        self.flops_per_transform = 2 * fd + 4 * f4  # one step: both DFTs and the four type-4 transforms
+        self.ops_per_step = 1
+        gen = torch.Generator(device=dev).manual_seed(5)
+        self.precs = []
+        for single in (False, True):
+            eng = minfft_b200.engine(single)
+            rdt = torch.float32 if single else torch.float64
+            cdt = torch.complex64 if single else torch.complex128
+            xs = [torch.randn(self.n_dft, dtype=cdt, device=dev, generator=gen) for _ in range(self.nsets)]
+            rs = [torch.randn(self.n_t4, dtype=rdt, device=dev, generator=gen) for _ in range(self.nsets)]
+            self.precs.append(dict(eng=eng, single=single, xs=xs, rs=rs,
+                                   y=torch.empty(self.n_dft, dtype=cdt, device=dev),
+                                   c=torch.empty(self.n_t4, dtype=rdt, device=dev),
+                                   s=torch.empty(self.n_t4, dtype=rdt, device=dev),
+                                   pd=eng.plan("dft", (self.n_dft,)), p4=eng.plan("t4", (self.n_t4,))))
+
+    def plans(self):
+        for p in self.precs:
+            yield p["eng"], p["pd"], ("dft",)
+            yield p["eng"], p["p4"], ("dct4", "dst4")
+
+    def rebuild(self, eng, plan):
+        for p in self.precs:
+            for key, fam, n in (("pd", "dft", self.n_dft), ("p4", "t4", self.n_t4)):
+                if p[key] is plan:
+                    plan.free()
+                    p[key] = eng.plan(fam, (n,))
+
+    def step(self, k):
+        s = k % self.nsets
+        for p in self.precs:
+            p["pd"]("dft", p["xs"][s].data_ptr(), p["y"].data_ptr(), check=False)
+            p["p4"]("dct4", p["rs"][s].data_ptr(), p["c"].data_ptr(), check=False)
+            p["p4"]("dst4", p["rs"][s].data_ptr(), p["s"].data_ptr(), check=False)
+
+    def check_errors(self):
+        for p in self.precs:
+            p["eng"].check()
+
+    def launches_per_step(self):
+        return sum(eng.launch_count(op, plan.aux) for eng, plan, ops in self.plans() for op in ops)
+
+    def e2e_setup(self):
+        t = self.torch
+        self.host = []
+        h2d = d2h = 0
+        for p in self.precs:
+            pin = lambda x: t.empty(x.shape, dtype=x.dtype, pin_memory=True)  # noqa: E731
+            h = dict(x=pin(p["xs"][0]), y=pin(p["y"]), r=pin(p["rs"][0]), c=pin(p["c"]), s=pin(p["s"]))
+            h["x"].copy_(p["xs"][0].cpu())
+            h["r"].copy_(p["rs"][0].cpu())
+            self.host.append(h)
+            h2d += h["x"].numel() * h["x"].element_size() + 2 * h["r"].numel() * h["r"].element_size()
+            d2h += h["y"].numel() * h["y"].element_size() + 2 * h["c"].numel() * h["c"].element_size()
+        return h2d, d2h
+
+    def e2e_step(self):
+        for p, h in zip(self.precs, self.host):
+            p["pd"]("dft", h["x"].data_ptr(), h["y"].data_ptr(), check=False)
+            p["p4"]("dct4", h["r"].data_ptr(), h["c"].data_ptr(), check=False)
+            p["p4"]("dst4", h["r"].data_ptr(), h["s"].data_ptr(), check=False)
+
+    def config(self):
+        return {"workload": "1-D dft 2^26 (c128, c64) + dct4/dst4 2^24 (f64, f32)",
+                "n_dft": self.n_dft, "n_t4": self.n_t4, "transforms_per_step": 6,
+                "flops": "5*N*log2(N) dft, 2.5*N*log2(N) dct4/dst4",
+                "inputs": "standard normal (torch generator seed 5)",
+                "l2": "inputs rotate over 2 sets (1.5 GiB per set), far beyond the 126 MB L2"}
+
+    @classmethod
+    def cpu_sample(cls, P):
+        return (f"{min(P, 4)} concurrent instances (one per OpenMP thread, own plans) of each transform of one step")
+
+    @classmethod
+    def cpu_measure(cls, kind, threads, warm, reps):
+        """A bounded sample: min(threads, 4) concurrent instances of each of
+        the six transforms (the 2^26 arrays take 1 GiB each)."""
+        P = min(threads, 4)
+        t = cpu_run(kind, (("dft", ("dft",), False), ("dft", ("dft",), True)), (cls.n_dft,), P, P, reps, warm)
+        t += cpu_run(kind, (("t4", ("dct4", "dst4"), False), ("t4", ("dct4", "dst4"), True)), (cls.n_t4,), P, P,
+                     reps, warm)
+        fd = 5.0 * cls.n_dft * math.log2(cls.n_dft)
+        f4 = 2.5 * cls.n_t4 * math.log2(cls.n_t4)
+        return t, (2 * fd + 4 * f4) * P * reps
+
+
+WORKLOADS = {"2d2048": Workload2D, "batch4096": WorkloadBatch4096, "mixed20000": WorkloadMixed,
+             "3d256": Workload3D256, "long1d": WorkloadLong1D}
 
 
 # -------------------------------------------------------------- CPU timing
@@ -486,6 +723,12 @@ def _ref_config(W):
         return {"workload": "20000 mixed 1-D transforms", "count": W.count, "log2n": "uniform integer 4..16",
                 "kinds": list(W.kinds), "precision": "f32",
                 "flops": "5*N*log2(N) dft, 2.5*N*log2(N) real-data kinds"}
+    if W.name == "3d256":
+        return {"workload": "3-D complex DFT 256x256x256 c64, forward then inverse", "dims": list(W.dims),
+                "precision": "f32 (reference single-precision build)", "flops": "5*N*log2(N) per transform, N=2^24"}
+    if W.name == "long1d":
+        return {"workload": "1-D dft 2^26 (c128, c64) + dct4/dst4 2^24 (f64, f32)", "n_dft": W.n_dft,
+                "n_t4": W.n_t4, "transforms_per_step": 6, "flops": "5*N*log2(N) dft, 2.5*N*log2(N) dct4/dst4"}
     cfg = {"workload": "2-D realdft->invrealdft and dct2->dct3 round trips, 2048x2048, f64 and f32",
            "dims": list(W.dims), "precisions": ["f64", "f32"], "transforms_per_step": 8,
            "flops": "2.5*N*log2(N) per transform, N=2^22"}
@@ -507,9 +750,13 @@ def run_engine(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    W = WORKLOADS[args.workload](torch, dev)
+    WC = WORKLOADS[args.workload]
+    if hasattr(WC, "precision"):
+        WC.precision = args.precision
+    W = WC(torch, dev)
     tuned = 0
-    if args.tune_file and all(os.path.exists(f"{args.tune_file}.{'f32' if s else 'f64'}") for s in (False, True)):
+    tune_path = lambda eng: f"{args.tune_file}.{'f32' if eng.single else 'f64'}"  # noqa: E731
+    if args.tune_file and list(W.plans()) and all(os.path.exists(tune_path(e)) for e, _, _ in W.plans()):
         # reuse a saved tuning table (e.g. for deterministic profiling runs)
         for eng, plan, ops in W.plans():
             eng.tune_load(f"{args.tune_file}.{'f32' if eng.single else 'f64'}")
@@ -535,10 +782,6 @@ def run_engine(args):
     torch.cuda.synchronize()
     W.check_errors()
 
-    # launch-level timing on during the timed region (events between launches)
-    for eng, plan, ops in W.plans():
-        eng.profile(plan.aux, args.steps * 8 + 64)
-
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     if dist:
@@ -559,6 +802,18 @@ def run_engine(args):
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
+
+    # the same steps again with launch-level timing (an event pair around
+    # every launch on the plan's stream): per-kernel durations for the
+    # roofline.  The events serialise consecutive launches, so these
+    # durations are upper bounds and this pass is not the headline number.
+    prof_steps = min(args.steps, 500)
+    for eng, plan, ops in W.plans():
+        eng.profile(plan.aux, prof_steps * 8 + 64)
+    torch.cuda.synchronize()
+    for k in range(prof_steps):
+        W.step(k)
+    torch.cuda.synchronize()
     flops_step = W.flops_per_transform * W.ops_per_step
     value = flops_step * args.steps * world / (ms / 1e3) / 1e9
 
@@ -569,6 +824,8 @@ def run_engine(args):
         for lab, cnt, tot, by in eng.profile_stats(plan.aux):
             stats.append((f"{prec} {lab}", cnt, tot, by))
         eng.profile(plan.aux, 0)
+    if not stats and hasattr(W, "roofline_stats"):
+        stats = W.roofline_stats(ms, args.steps)  # one launch per step: the timed region itself
     stats.sort(key=lambda r: -r[2])
     hbm, peak_src = peaks()
     roof = None
@@ -621,11 +878,15 @@ def run_engine(args):
     if rank == 0 and world == 1 and not args.no_cpu and hasattr(W, "cpu_measure"):
         P = cpu_threads()
         kind = cpu_kind()
-        t, flops = W.cpu_measure(kind, P, 1, 1)
+        reps = 1
+        t, flops = W.cpu_measure(kind, P, 1, reps)
+        if t < 5.0:  # a short sample: repeat it to about 10 s of CPU work
+            reps = min(100, int(math.ceil(10.0 / max(t, 1e-3))))
+            t, flops = W.cpu_measure(kind, P, 1, reps)
         cpu = {"value": round(flops / t / 1e9, 3), "unit": "GFLOP/s", "cores": P, "kind": kind,
                "sample": (W.cpu_sample(P) if hasattr(W, "cpu_sample") else
                           f"{P} concurrent independent instances of one step (one per OpenMP thread, own plans)")
-               + f", {t:.1f} s"}
+               + f", {reps} timed repetition(s), {t:.1f} s"}
 
     if rank == 0:
         line = {"metric": "GFLOP/s (5N log2N complex, 2.5N log2N real-data)", "value": round(value, 3),
@@ -646,7 +907,7 @@ def run_engine(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="2d2048")
@@ -654,6 +915,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (heuristic launch configurations)")
     ap.add_argument("--tune-file", default="", help="tuning table prefix: loaded if present, else saved after tuning")
+    ap.add_argument("--precision", choices=["fp32", "tc_f16", "tc_bf16"], default="fp32",
+                    help="3d256: arithmetic of the 256-point axis passes")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -686,6 +686,8 @@ template <int L, int R, class LoadOp, class StoreOp>
 __global__ void __launch_bounds__(512, MinBlocks<R>::value) axis_pass_kernel(const AxisParams p) {
   static_assert(R <= L || L < 2, "radix at most the length");
   constexpr int TPT = L / R;
+  pdl_release();
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   int64_t* offs = reinterpret_cast<int64_t*>(smem_raw);
   const int64_t left = p.nbatch - int64_t(blockIdx.x) * p.cpb;

@@ -131,6 +131,16 @@ __device__ __forceinline__ void fft_reg(cpx* v) {
   }
 }
 
+// ------------------------------------------------ programmatic dependent launch
+// A kernel enqueued with the programmatic stream-serialization attribute may
+// be scheduled while the kernel before it drains.  pdl_wait() blocks until
+// that predecessor grid has completed and its writes are visible (a no-op
+// for an ordinary launch); pdl_release() allows the next kernel to be
+// scheduled once every CTA of this grid has called it or exited.  Every
+// kernel the planner launches calls both before touching global memory.
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // --------------------------------------------------------------- misc utils
 __device__ __forceinline__ int pad16(int p) { return p + (p >> 4); }
 __host__ __device__ constexpr int padded_len(int L) { return L + (L >> 4); }

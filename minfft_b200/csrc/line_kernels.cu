@@ -10,6 +10,8 @@ namespace {
 
 template <class Op>
 __global__ void k_line(const LineParams p) {
+  pdl_release();
+  pdl_wait();
   const int64_t total = Op::count(p);
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
     Op::item(p, e);

@@ -230,6 +230,8 @@ __global__ void __launch_bounds__(512, MinBlocks<R>::value) axis_pipe_kernel(con
   constexpr int TPT = L / R;
   using Raw = typename PLoad::Raw;
   constexpr int ER = PLoad::e_raw(L);
+  pdl_release();
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   int64_t* offs = reinterpret_cast<int64_t*>(smem_raw);  // [stage][in|out][cpb]
   unsigned char* stages = smem_raw + pipe_offsets_bytes(p.cpb);

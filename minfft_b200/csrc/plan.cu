@@ -1186,6 +1186,33 @@ struct DeviceGuard {
   }
 };
 
+// Programmatic dependent launch for the planner's kernels (every one of them
+// starts with pdl_release / pdl_wait): consecutive launches of a program
+// overlap the next kernel's scheduling with the previous one's drain.
+// MINFFT_B200_PDL=0 turns it off.
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MINFFT_B200_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+bool enqueue(minfft_aux* a, const Launch& ln, void** args, size_t smem, const char* what) {
+  if (!pdl_enabled()) return cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, smem, a->stream), what);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ln.grid);
+  cfg.blockDim = dim3(ln.block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = a->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cuda_ok(cudaLaunchKernelExC(&cfg, ln.fn, args), what);
+}
+
 // Enqueue one planned launch with its buffers resolved.
 bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
   void* args[1];
@@ -1194,7 +1221,7 @@ bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
     lp.in = bufs[ln.in_buf];
     lp.out = bufs[ln.out_buf];
     args[0] = &lp;
-    return cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, 0, a->stream), "launch(line)");
+    return enqueue(a, ln, args, 0, "launch(line)");
   }
   AxisParams ap = ln.ap;
   ap.in = bufs[ln.in_buf];
@@ -1209,10 +1236,10 @@ bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
   if (ln.tc) {
     mb::TcParams tcp = ln.tcp;
     void* targs[2] = {&ap, &tcp};
-    return cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), targs, ln.smem, a->stream), "launch(tc)");
+    return enqueue(a, ln, targs, ln.smem, "launch(tc)");
   }
   args[0] = &ap;
-  return cuda_ok(cudaLaunchKernel(ln.fn, dim3(ln.grid), dim3(ln.block), args, ln.smem, a->stream), "launch(axis)");
+  return enqueue(a, ln, args, ln.smem, "launch(axis)");
 }
 
 bool run_program(minfft_aux* a, Program* prog, void* x, void* y) {

@@ -239,6 +239,8 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
+  pdl_release();
+  pdl_wait();
   const uint32_t mbar_a = static_cast<uint32_t>(__cvta_generic_to_shared(mbar));
   const int64_t ntiles = (p.nbatch + TB - 1) / TB;
   if (warp == 0) {
