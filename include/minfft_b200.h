@@ -151,15 +151,19 @@ enum {
 };
 int minfft_b200_set_precision(minfft_aux *a, int mode);
 int minfft_b200_get_precision(const minfft_aux *a);
-/* Waits for plan `a`'s stream and reports whether a tensor-core pass gave up
- * waiting for its matrix units (MINFFT_B200_ETIMEOUT; that pass's output is
- * then incomplete) since the previous call; clears the record. */
+/* Waits for plan `a`'s stream and reports whether one of its kernels gave up
+ * on a bounded device-side wait (a tensor-core pass waiting for its matrix
+ * operations) since the previous call: MINFFT_B200_ETIMEOUT, and that
+ * launch's output is incomplete.  Clears the record.  minfft_b200_tc_status
+ * is the same call. */
+int minfft_b200_device_status(const minfft_aux *a);
 int minfft_b200_tc_status(const minfft_aux *a);
 
 /* ------------------------------------------------------------- autotuner */
 /* Time the candidate launch configurations (kernel form: one tile per CTA
  * or persistent CTAs with double-buffered asynchronous copies; per-thread
- * radix 8 or 16; transforms per CTA) of every kernel launch of transform `op` on `howmany` arrays of plan
+ * radix 8 or 16; transforms per CTA) of every kernel launch of transform `op`
+ * on `howmany` arrays of plan
  * `a`, using scratch buffers (`reps` timed runs each), and keep the fastest
  * in a process-wide table that every plan consults when it builds its launch
  * lists.  The table can be saved to and loaded from a text file. */

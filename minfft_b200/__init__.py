@@ -89,6 +89,8 @@ class Engine(MinfftLibrary):
         L.minfft_b200_get_precision.restype = i32
         L.minfft_b200_tc_status.argtypes = [vp]
         L.minfft_b200_tc_status.restype = i32
+        L.minfft_b200_device_status.argtypes = [vp]
+        L.minfft_b200_device_status.restype = i32
         L.minfft_b200_autotune.argtypes = [vp, i32, i32, i32]
         L.minfft_b200_autotune.restype = i32
         for f in ("minfft_b200_tune_save", "minfft_b200_tune_load"):
@@ -163,6 +165,11 @@ class Engine(MinfftLibrary):
     def get_precision(self, aux: int) -> str:
         code = int(self.lib.minfft_b200_get_precision(ctypes.c_void_p(aux)))
         return {v: k for k, v in PRECISIONS.items()}[code]
+
+    def device_status(self, aux: int) -> None:
+        """Raise if a kernel of the plan gave up on a bounded device-side wait since the last call."""
+        if self.lib.minfft_b200_device_status(ctypes.c_void_p(aux)):
+            self.check()
 
     def tc_status(self, aux: int) -> None:
         """Raise if a tensor-core pass of the plan gave up waiting since the last call."""

@@ -52,6 +52,7 @@ struct AxisParams {
   int64_t gpb;          // pipelined kernel, column mode: tiles per d0 block
   int stage_bytes;      // pipelined kernel: bytes of one shared-memory stage
   int lp;               // shared-memory pitch between transforms (tile_pitch)
+  int* status;          // set to 1 by a kernel whose bounded device-side wait ran out
 };
 
 enum : int {

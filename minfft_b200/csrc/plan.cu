@@ -277,7 +277,8 @@ struct minfft_aux {
   size_t buf_bytes[BUF_COUNT] = {0, 0, 0, 0, 0, 0};
   std::map<std::tuple<int, int, int>, Program> programs;  // (op, howmany, alias)
   int precision = MINFFT_B200_PREC_FP32;  // arithmetic of the 256-point complex passes
-  void* tc_mem = nullptr;                 // tensor-core B operands (both formats) and status word
+  void* tc_mem = nullptr;                 // tensor-core B operands (both formats)
+  int* dev_status = nullptr;              // set by kernels whose bounded device-side wait ran out
   void* stage_in = nullptr;
   size_t stage_in_bytes = 0;
   void* stage_out = nullptr;
@@ -503,8 +504,7 @@ struct Planner {
         return;
       }
       ln.tcp.bmat = static_cast<const char*>(a->tc_mem) + (fmt == mb::TC_F16 ? 0 : mb::tc_bmat_bytes(mb::TC_F16));
-      ln.tcp.status = reinterpret_cast<int*>(static_cast<char*>(a->tc_mem) + mb::tc_bmat_bytes(mb::TC_F16) +
-                                             mb::tc_bmat_bytes(mb::TC_BF16));
+      ln.tcp.status = a->dev_status;
     }
     ap.cpb = tb;
     ap.nbatch = nbatch;
@@ -655,8 +655,9 @@ struct Planner {
       if (cpb < want) cpb = std::max(cpb, std::min(want, std::max(1, 512 / tpt)));
     }
     const int er = mb::pipe_raw_elems(combo, L);
-    while (cpb > 1 && mb::pipe_smem(L, R, cpb, colmode ? 1 : 0, er, mb::pipe_raw_size(combo)) > (size_t)dev_max_smem)
-      cpb /= 2;
+    const size_t esz = mb::pipe_raw_size(combo);
+    auto smem = [&](int c) { return mb::pipe_smem(L, R, c, colmode ? 1 : 0, er, esz); };
+    while (cpb > 1 && smem(cpb) > (size_t)dev_max_smem) cpb /= 2;
     return cpb;
   }
 
@@ -1226,6 +1227,7 @@ bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
   AxisParams ap = ln.ap;
   ap.in = bufs[ln.in_buf];
   ap.out = bufs[ln.out_buf];
+  ap.status = a->dev_status;
   if (ln.vec_in && (reinterpret_cast<uintptr_t>(ap.in) % sizeof(cpx)) == 0) ap.flags |= mb::F_VEC;
   if (ln.vec_out && (reinterpret_cast<uintptr_t>(ap.out) % sizeof(cpx)) == 0) ap.flags |= mb::F_VEC;
   if (ln.pipe) {
@@ -1390,6 +1392,15 @@ minfft_aux* make_plan(int family, int d, const int* Ns) {
     delete a;
     return nullptr;
   }
+  {
+    void* st = nullptr;
+    if (!cuda_ok(cudaMalloc(&st, 16), "cudaMalloc(status)") || !cuda_ok(cudaMemset(st, 0, 16), "cudaMemset(status)")) {
+      if (st) cudaFree(st);
+      delete a;
+      return nullptr;
+    }
+    a->dev_status = static_cast<int*>(st);
+  }
   // plan every transform of the family (out of place, one array) now, so
   // tables and scratch are allocated up front as the reference's makers do
   static const int fam_ops[4][4] = {{MINFFT_B200_DFT, MINFFT_B200_INVDFT, -1, -1},
@@ -1420,6 +1431,7 @@ MB_EXPORT void minfft_free_aux(minfft_aux* a) {
     if (a->stage_in) cudaFree(a->stage_in);
     if (a->stage_out) cudaFree(a->stage_out);
     if (a->tc_mem) cudaFree(a->tc_mem);
+    if (a->dev_status) cudaFree(a->dev_status);
     for (cudaEvent_t e : a->ev_pool) cudaEventDestroy(e);
   }
   delete a;
@@ -1552,26 +1564,27 @@ MB_EXPORT int minfft_b200_set_precision(minfft_aux* a, int mode) {
 
 MB_EXPORT int minfft_b200_get_precision(const minfft_aux* a) { return a ? a->precision : -1; }
 
-MB_EXPORT int minfft_b200_tc_status(const minfft_aux* ca) {
+MB_EXPORT int minfft_b200_device_status(const minfft_aux* ca) {
   if (!ca) {
     set_error(MINFFT_B200_EINVAL, "NULL plan");
     return MINFFT_B200_EINVAL;
   }
-  if (!ca->tc_mem) return MINFFT_B200_OK;
+  if (!ca->dev_status) return MINFFT_B200_OK;
   DeviceGuard guard(ca->device);
   if (!cuda_ok(cudaStreamSynchronize(ca->stream), "cudaStreamSynchronize")) return g_err;
-  int* st = reinterpret_cast<int*>(static_cast<char*>(ca->tc_mem) + mb::tc_bmat_bytes(mb::TC_F16) +
-                                   mb::tc_bmat_bytes(mb::TC_BF16));
   int v = 0;
-  if (!cuda_ok(cudaMemcpy(&v, st, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(tc status)")) return g_err;
+  if (!cuda_ok(cudaMemcpy(&v, ca->dev_status, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(status)"))
+    return g_err;
   if (v) {
     const int zero = 0;
-    cudaMemcpy(st, &zero, sizeof(int), cudaMemcpyHostToDevice);
-    set_error(MINFFT_B200_ETIMEOUT, "a tensor-core pass gave up waiting for its matrix operations");
+    cudaMemcpy(ca->dev_status, &zero, sizeof(int), cudaMemcpyHostToDevice);
+    set_error(MINFFT_B200_ETIMEOUT, "a kernel gave up waiting on a device-side barrier");
     return MINFFT_B200_ETIMEOUT;
   }
   return MINFFT_B200_OK;
 }
+
+MB_EXPORT int minfft_b200_tc_status(const minfft_aux* ca) { return minfft_b200_device_status(ca); }
 
 MB_EXPORT int minfft_b200_profile(minfft_aux* a, int enable) {
   if (!a) {

@@ -336,7 +336,8 @@ def test_autotuned_plans_stay_correct(single, tmp_path):
 def test_every_forced_configuration_is_correct(single, pipe, radix):
     """Both kernel forms, both per-thread radices, at every tile size
     (transforms per CTA), forced as the default configuration, on row and
-    column passes of every transform kind."""
+    column passes of every transform kind, including the 1025 columns of a
+    2-D real DFT."""
     eng = minfft_b200.engine(single)
     rng = np.random.default_rng(43)
     saved = eng.tune_size()
@@ -344,7 +345,7 @@ def test_every_forced_configuration_is_correct(single, pipe, radix):
         eng.tune_clear()
         for cpb in (1, 2, 4, 8, 16, 64):
             eng.tune_set_default(pipe, cpb, radix)
-            for dims in [(64, 512), (8, 2048), (1 << 14,)]:
+            for dims in [(64, 512), (8, 2048), (1 << 14,), (16, 2048)]:
                 for op in OPS:
                     x = make_input(op, dims, rng, single)
                     err = rel_l2(gpu_apply(op, x, dims, single), expected(op, x, dims))
@@ -352,3 +353,4 @@ def test_every_forced_configuration_is_correct(single, pipe, radix):
     finally:
         eng.tune_set_default(-1, 0, 16)
     assert saved >= 0
+
