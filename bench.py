@@ -221,8 +221,17 @@ class Workload2D:
         return tot
 
     def e2e_setup(self):
-        """Pinned host copies of one input set and host outputs."""
+        """Pinned host copies of one input set and host outputs; every plan on
+        its own stream in host-async mode, so the four plans' uploads,
+        transforms and downloads overlap within a step."""
         torch = self.torch
+        self.e2e_plans = []
+        for p in self.precs:
+            for key in ("pr", "pt"):
+                st = torch.cuda.Stream()
+                p[key].set_stream(st.cuda_stream)
+                p[key].set_host_async(True)
+                self.e2e_plans.append((p[key], st))
         self.host = []
         for p in self.precs:
             pin = lambda t: torch.empty(t.shape, dtype=t.dtype, pin_memory=True)  # noqa: E731
@@ -245,6 +254,8 @@ class Workload2D:
             pr("invrealdft", h["z"].data_ptr(), h["x2"].data_ptr(), check=False)
             pt("dct2", h["x"].data_ptr(), h["c"].data_ptr(), check=False)
             pt("dct3", h["c"].data_ptr(), h["x3"].data_ptr(), check=False)
+        for plan, _ in self.e2e_plans:
+            plan.synchronize()
 
     def config(self):
         return {"workload": "2-D realdft->invrealdft and dct2->dct3 round trips, 2048x2048, f64 and f32",
@@ -373,28 +384,38 @@ class WorkloadMixed:
         self.ops, self.ns = self.job_list()
         self.eng = minfft_b200.engine(True)
         esz = 4
+        # all inputs in one region of the pool, all outputs in the next
+        # (256-byte aligned slices), so a step's upload and download are one
+        # contiguous copy each
         offs_in, offs_out, tot = [], [], 0
         self.in_bytes = self.out_bytes = 0
+        sizes = []
         for op, n in zip(self.ops, self.ns):
             ins, inc, outs, outc = shapes(op, (n,))
-            bi = int(np.prod(ins)) * esz * (2 if inc else 1)
-            bo = int(np.prod(outs)) * esz * (2 if outc else 1)
+            sizes.append((int(np.prod(ins)) * esz * (2 if inc else 1), int(np.prod(outs)) * esz * (2 if outc else 1)))
+        for bi, _ in sizes:
             offs_in.append((tot, bi))
             tot += (bi + 255) // 256 * 256
+            self.in_bytes += bi
+        self.in_region = tot
+        for _, bo in sizes:
             offs_out.append((tot, bo))
             tot += (bo + 255) // 256 * 256
-            self.in_bytes += bi
             self.out_bytes += bo
-        self.pool = torch.empty(tot // 4 + 64, dtype=torch.float32, device=dev)
+        self.pool_elems = tot // 4 + 64
+        self.pool = torch.empty(self.pool_elems, dtype=torch.float32, device=dev)
         self.pool.normal_(generator=torch.Generator(device=dev).manual_seed(4))
-        base = self.pool.data_ptr()
-        self.jobs = [(op, n, base + oi, base + oo) for op, n, (oi, _), (oo, _) in zip(self.ops, self.ns, offs_in,
-                                                                                       offs_out)]
         self.offs_in, self.offs_out = offs_in, offs_out
-        self.handle = self.eng.mixed_plan(self.jobs)
+        self.dev = dev
+        self.handle = self.eng.mixed_plan(self._jobs(self.pool))
         self.flops_per_transform = sum((5.0 if op == "dft" else 2.5) * n * math.log2(n)
                                        for op, n in zip(self.ops, self.ns))
         self.ops_per_step = 1
+
+    def _jobs(self, pool):
+        base = pool.data_ptr()
+        return [(op, n, base + oi, base + oo) for op, n, (oi, _), (oo, _) in zip(self.ops, self.ns, self.offs_in,
+                                                                               self.offs_out)]
 
     def plans(self):
         return iter(())
@@ -421,18 +442,34 @@ class WorkloadMixed:
         return [("f32 mixed_kernel (graph launch)", steps, ms, float(self.in_bytes + self.out_bytes))]
 
     def e2e_setup(self):
+        """Two device pools with their own plans and streams, used on
+        alternate steps: a step uploads its inputs (one copy of the input
+        region from pinned host memory), launches the graph and downloads its
+        outputs (one copy of the output region), all on its stream, so one
+        step's upload overlaps the previous step's download."""
         t = self.torch
-        self.hpool = t.empty(self.pool.shape, dtype=t.float32, pin_memory=True)
-        self.hpool.copy_(self.pool.cpu())
-        nb = self.pool.numel() * 4  # the whole pool (inputs and outputs) goes each way
-        return nb, nb
+        self.pool_b = t.empty(self.pool_elems, dtype=t.float32, device=self.dev)
+        self.pool_b.copy_(self.pool)
+        self.handle_b = self.eng.mixed_plan(self._jobs(self.pool_b))
+        self.eng.mixed_autotune(self.handle_b, 3)
+        self.slots = [(self.pool, self.handle, t.cuda.Stream()), (self.pool_b, self.handle_b, t.cuda.Stream())]
+        ni = self.in_region // 4
+        self.h_in = t.empty(ni, dtype=t.float32, pin_memory=True)
+        self.h_in.copy_(self.pool[:ni].cpu())
+        self.h_out = [t.empty(self.pool_elems - ni, dtype=t.float32, pin_memory=True) for _ in range(2)]
+        self.e2e_k = 0
+        return ni * 4, (self.pool_elems - ni) * 4
 
     def e2e_step(self):
-        # inputs in, one graph launch, outputs back (pinned host pool)
-        self.pool.copy_(self.hpool, non_blocking=True)
-        self.eng.mixed_execute(self.handle)
-        self.hpool.copy_(self.pool, non_blocking=True)
-        self.torch.cuda.synchronize()
+        t = self.torch
+        i = self.e2e_k & 1
+        self.e2e_k += 1
+        pool, handle, st = self.slots[i]
+        ni = self.in_region // 4
+        with t.cuda.stream(st):
+            pool[:ni].copy_(self.h_in, non_blocking=True)
+            self.eng.mixed_execute(handle, st.cuda_stream)
+            self.h_out[i].copy_(pool[ni:], non_blocking=True)
 
     def config(self):
         return {"workload": "20000 mixed 1-D transforms, one persistent graph-launched kernel",
@@ -602,6 +639,13 @@ class WorkloadLong1D:
     def e2e_setup(self):
         t = self.torch
         self.host = []
+        self.e2e_plans = []
+        for p in self.precs:
+            for key in ("pd", "p4"):
+                st = t.cuda.Stream()
+                p[key].set_stream(st.cuda_stream)
+                p[key].set_host_async(True)
+                self.e2e_plans.append((p[key], st))
         h2d = d2h = 0
         for p in self.precs:
             pin = lambda x: t.empty(x.shape, dtype=x.dtype, pin_memory=True)  # noqa: E731
@@ -618,6 +662,8 @@ class WorkloadLong1D:
             p["pd"]("dft", h["x"].data_ptr(), h["y"].data_ptr(), check=False)
             p["p4"]("dct4", h["r"].data_ptr(), h["c"].data_ptr(), check=False)
             p["p4"]("dst4", h["r"].data_ptr(), h["s"].data_ptr(), check=False)
+        for plan, _ in self.e2e_plans:
+            plan.synchronize()
 
     def config(self):
         return {"workload": "1-D dft 2^26 (c128, c64) + dct4/dst4 2^24 (f64, f32)",
@@ -855,6 +901,7 @@ def run_engine(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         W.e2e_step()
+        torch.cuda.synchronize()
         est = time.perf_counter() - t0
         k_e2e = max(3, min(args.steps, int(5.0 / max(est, 1e-4))))
         if dist:

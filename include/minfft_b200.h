@@ -44,6 +44,17 @@ int minfft_b200_set_stream(minfft_aux *a, void *stream);
 void *minfft_b200_get_stream(const minfft_aux *a);
 int minfft_b200_synchronize(const minfft_aux *a);
 
+/* Host-async mode (off by default; no counterpart in the reference, whose
+ * calls return when the output is ready).  With enable != 0, a call on plan
+ * `a` whose input and output are both page-locked host arrays (cudaHostAlloc
+ * or cudaHostRegister) or device arrays is enqueued on the plan's stream --
+ * upload, kernels, download -- and returns at once; the caller waits with
+ * minfft_b200_synchronize(a) (or the stream) before reading the output or
+ * overwriting the input.  Calls on pageable host memory stay synchronous.
+ * Consecutive calls on one plan reuse its staging buffers in stream order,
+ * so plans on different streams overlap their copies in both directions. */
+int minfft_b200_set_host_async(minfft_aux *a, int enable);
+
 /* ------------------------------------------------------------ transforms */
 /* Transform codes for the generic entry points below. */
 enum {

@@ -91,6 +91,8 @@ class Engine(MinfftLibrary):
         L.minfft_b200_tc_status.restype = i32
         L.minfft_b200_device_status.argtypes = [vp]
         L.minfft_b200_device_status.restype = i32
+        L.minfft_b200_set_host_async.argtypes = [vp, i32]
+        L.minfft_b200_set_host_async.restype = i32
         L.minfft_b200_autotune.argtypes = [vp, i32, i32, i32]
         L.minfft_b200_autotune.restype = i32
         for f in ("minfft_b200_tune_save", "minfft_b200_tune_load"):
@@ -165,6 +167,11 @@ class Engine(MinfftLibrary):
     def get_precision(self, aux: int) -> str:
         code = int(self.lib.minfft_b200_get_precision(ctypes.c_void_p(aux)))
         return {v: k for k, v in PRECISIONS.items()}[code]
+
+    def set_host_async(self, aux: int, enable: bool = True) -> None:
+        """Page-locked host arrays: calls return at once, ordered on the plan's stream."""
+        if self.lib.minfft_b200_set_host_async(ctypes.c_void_p(aux), int(bool(enable))):
+            self.check()
 
     def device_status(self, aux: int) -> None:
         """Raise if a kernel of the plan gave up on a bounded device-side wait since the last call."""
@@ -269,6 +276,12 @@ class Plan:
 
     def set_stream(self, stream: int) -> None:
         self.engine.set_stream(self.aux, stream)
+
+    def set_host_async(self, enable: bool = True) -> None:
+        self.engine.set_host_async(self.aux, enable)
+
+    def synchronize(self) -> None:
+        self.engine.synchronize(self.aux)
 
     def free(self) -> None:
         if self.aux:

@@ -279,6 +279,7 @@ struct minfft_aux {
   int precision = MINFFT_B200_PREC_FP32;  // arithmetic of the 256-point complex passes
   void* tc_mem = nullptr;                 // tensor-core B operands (both formats)
   int* dev_status = nullptr;              // set by kernels whose bounded device-side wait ran out
+  bool host_async = false;                // page-locked host arrays: stream-ordered calls (minfft_b200_set_host_async)
   void* stage_in = nullptr;
   size_t stage_in_bytes = 0;
   void* stage_out = nullptr;
@@ -1167,13 +1168,16 @@ Program* get_program(minfft_aux* a, int op, int howmany, bool alias) {
   return &(a->programs[key] = std::move(prog));
 }
 
-bool is_device_pointer(const void* p) {
+enum PtrKind { PTR_PAGEABLE = 0, PTR_PINNED, PTR_DEVICE };
+
+PtrKind pointer_kind(const void* p) {
   cudaPointerAttributes attr;
   if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return PTR_PAGEABLE;
   }
-  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+  if (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) return PTR_DEVICE;
+  return attr.type == cudaMemoryTypeHost ? PTR_PINNED : PTR_PAGEABLE;
 }
 
 struct DeviceGuard {
@@ -1331,7 +1335,12 @@ int execute(int op, void* x, void* y, int howmany, const minfft_aux* ca) {
   DeviceGuard guard(a->device);
   const size_t in_b = size_t(io_bytes(a, op, false)) * howmany;
   const size_t out_b = size_t(io_bytes(a, op, true)) * howmany;
-  const bool x_dev = is_device_pointer(x), y_dev = is_device_pointer(y);
+  const PtrKind xk = pointer_kind(x), yk = pointer_kind(y);
+  const bool x_dev = xk == PTR_DEVICE, y_dev = yk == PTR_DEVICE;
+  // host arrays are staged through device buffers; the call waits for its
+  // result unless the plan is in host-async mode and both arrays are
+  // page-locked (then everything stays ordered on the plan's stream)
+  const bool wait_host = !(a->host_async && xk != PTR_PAGEABLE && yk != PTR_PAGEABLE);
   void* dx = x;
   void* dy = y;
   const bool same = (x == y);
@@ -1357,7 +1366,7 @@ int execute(int op, void* x, void* y, int howmany, const minfft_aux* ca) {
   if (!y_dev) {
     if (!cuda_ok(cudaMemcpyAsync(y, dy, out_b, cudaMemcpyDeviceToHost, a->stream), "cudaMemcpyAsync(D2H)"))
       return g_err;
-    if (!cuda_ok(cudaStreamSynchronize(a->stream), "cudaStreamSynchronize")) return g_err;
+    if (wait_host && !cuda_ok(cudaStreamSynchronize(a->stream), "cudaStreamSynchronize")) return g_err;
   }
   return MINFFT_B200_OK;
 }
@@ -1563,6 +1572,15 @@ MB_EXPORT int minfft_b200_set_precision(minfft_aux* a, int mode) {
 }
 
 MB_EXPORT int minfft_b200_get_precision(const minfft_aux* a) { return a ? a->precision : -1; }
+
+MB_EXPORT int minfft_b200_set_host_async(minfft_aux* a, int enable) {
+  if (!a) {
+    set_error(MINFFT_B200_EINVAL, "NULL plan");
+    return MINFFT_B200_EINVAL;
+  }
+  a->host_async = enable != 0;
+  return MINFFT_B200_OK;
+}
 
 MB_EXPORT int minfft_b200_device_status(const minfft_aux* ca) {
   if (!ca) {

@@ -354,3 +354,53 @@ def test_every_forced_configuration_is_correct(single, pipe, radix):
         eng.tune_set_default(-1, 0, 16)
     assert saved >= 0
 
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+def test_host_async_mode(single):
+    """Host-async mode: calls on page-locked host arrays are ordered on the
+    plan's stream and return at once; plans on their own streams run
+    concurrently; after synchronizing, every output matches the oracle.
+    Pageable arrays keep the synchronous behaviour."""
+    eng = minfft_b200.engine(single)
+    rng = np.random.default_rng(45)
+    rdt, cdt = oracle.np_dtypes(single)
+    dims = (256, 512)
+    ops = [("realdft", "invrealdft"), ("dct2", "dct3")]
+    plans, streams, jobs = [], [], []
+    try:
+        for first, second in ops:
+            plan = eng.plan(OP_FAMILY[first], dims)
+            st = torch.cuda.Stream()
+            plan.set_stream(st.cuda_stream)
+            plan.set_host_async(True)
+            plans.append(plan)
+            streams.append(st)
+            x = make_input(first, dims, rng, single)
+            _, _, s1, c1 = shapes(first, dims)
+            _, _, s2, c2 = shapes(second, dims)
+            tdt = lambda c: {np.float32: torch.float32, np.float64: torch.float64, np.complex64: torch.complex64,
+                             np.complex128: torch.complex128}[cdt if c else rdt]  # noqa: E731
+            hx = torch.from_numpy(x).pin_memory()
+            h1 = torch.empty(s1, dtype=tdt(c1)).pin_memory()
+            h2 = torch.empty(s2, dtype=tdt(c2)).pin_memory()
+            jobs.append((plan, first, second, x, hx, h1, h2))
+        for plan, first, second, x, hx, h1, h2 in jobs:
+            plan(first, hx.data_ptr(), h1.data_ptr())
+            plan(second, h1.data_ptr(), h2.data_ptr())
+        for plan in plans:
+            plan.synchronize()
+        for plan, first, second, x, hx, h1, h2 in jobs:
+            y1 = expected(first, x, dims)
+            assert rel_l2(h1.numpy(), y1) <= tolerance(single, dims), first
+            y2 = expected(second, y1.astype(cdt if np.iscomplexobj(y1) else rdt), dims)
+            assert rel_l2(h2.numpy(), y2) <= 4 * tolerance(single, dims), second
+        # pageable arrays in host-async mode: still synchronous
+        plan, first, second, x = jobs[0][0], jobs[0][1], jobs[0][2], jobs[0][3]
+        _, _, s1, c1 = shapes(first, dims)
+        y = np.zeros(s1, dtype=cdt if c1 else rdt)
+        plan(first, np.ascontiguousarray(x).ctypes.data, y.ctypes.data)
+        assert rel_l2(y, expected(first, x, dims)) <= tolerance(single, dims)
+    finally:
+        for plan in plans:
+            plan.free()
