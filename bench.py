@@ -221,41 +221,56 @@ class Workload2D:
         return tot
 
     def e2e_setup(self):
-        """Pinned host copies of one input set and host outputs; every plan on
-        its own stream in host-async mode, so the four plans' uploads,
-        transforms and downloads overlap within a step."""
+        """Pinned host copies of one input set and two sets of plans and host
+        outputs, used on alternate steps.  Every plan has its own stream in
+        host-async mode, so within a step the four plans' uploads, transforms
+        and downloads overlap, and a step's uploads overlap the previous
+        step's downloads; a set waits for its own previous step (two steps
+        back) before it is reused."""
         torch = self.torch
-        self.e2e_plans = []
+        pin = lambda t: torch.empty(t.shape, dtype=t.dtype, pin_memory=True)  # noqa: E731
+        self.e2e_sets = []
+        for k in range(2):
+            plans, host = [], []
+            for p in self.precs:
+                pr = p["pr"] if k == 0 else p["eng"].plan("realdft", self.dims)
+                pt = p["pt"] if k == 0 else p["eng"].plan("t2t3", self.dims)
+                streams = []
+                for plan in (pr, pt):
+                    st = torch.cuda.Stream()
+                    plan.set_stream(st.cuda_stream)
+                    plan.set_host_async(True)
+                    streams.append(st)
+                plans.append((pr, pt, streams))
+                host.append(dict(z=pin(p["z"]), x2=pin(p["x2"]), c=pin(p["c"]), x3=pin(p["x3"])))
+            self.e2e_sets.append((plans, host))
+        self.hx = []
         for p in self.precs:
-            for key in ("pr", "pt"):
-                st = torch.cuda.Stream()
-                p[key].set_stream(st.cuda_stream)
-                p[key].set_host_async(True)
-                self.e2e_plans.append((p[key], st))
-        self.host = []
-        for p in self.precs:
-            pin = lambda t: torch.empty(t.shape, dtype=t.dtype, pin_memory=True)  # noqa: E731
             hx = pin(p["xs"][0])
             hx.copy_(p["xs"][0].cpu())
-            self.host.append(dict(x=hx, z=pin(p["z"]), x2=pin(p["x2"]), c=pin(p["c"]), x3=pin(p["x3"])))
+            self.hx.append(hx)
+        self.e2e_k = 0
         h2d = d2h = 0
-        for h in self.host:
+        for hx, h in zip(self.hx, self.e2e_sets[0][1]):
             # each call stages its input to the device and its output back
-            h2d += 2 * h["x"].numel() * h["x"].element_size() + h["z"].numel() * h["z"].element_size() + \
+            h2d += 2 * hx.numel() * hx.element_size() + h["z"].numel() * h["z"].element_size() + \
                 h["c"].numel() * h["c"].element_size()
             d2h += h["z"].numel() * h["z"].element_size() + h["x2"].numel() * h["x2"].element_size() + \
                 h["c"].numel() * h["c"].element_size() + h["x3"].numel() * h["x3"].element_size()
         return h2d, d2h
 
     def e2e_step(self):
-        for p, h in zip(self.precs, self.host):
-            pr, pt = p["pr"], p["pt"]
-            pr("realdft", h["x"].data_ptr(), h["z"].data_ptr(), check=False)
+        plans, host = self.e2e_sets[self.e2e_k & 1]
+        if self.e2e_k >= 2:
+            for pr, pt, _ in plans:
+                pr.synchronize()
+                pt.synchronize()
+        self.e2e_k += 1
+        for (pr, pt, _), hx, h in zip(plans, self.hx, host):
+            pr("realdft", hx.data_ptr(), h["z"].data_ptr(), check=False)
             pr("invrealdft", h["z"].data_ptr(), h["x2"].data_ptr(), check=False)
-            pt("dct2", h["x"].data_ptr(), h["c"].data_ptr(), check=False)
+            pt("dct2", hx.data_ptr(), h["c"].data_ptr(), check=False)
             pt("dct3", h["c"].data_ptr(), h["x3"].data_ptr(), check=False)
-        for plan, _ in self.e2e_plans:
-            plan.synchronize()
 
     def config(self):
         return {"workload": "2-D realdft->invrealdft and dct2->dct3 round trips, 2048x2048, f64 and f32",
@@ -637,33 +652,49 @@ class WorkloadLong1D:
         return sum(eng.launch_count(op, plan.aux) for eng, plan, ops in self.plans() for op in ops)
 
     def e2e_setup(self):
+        """Two sets of plans (each on its own streams, host-async mode) and
+        host outputs used on alternate steps, as in the 2-D workload."""
         t = self.torch
-        self.host = []
-        self.e2e_plans = []
+        pin = lambda x: t.empty(x.shape, dtype=x.dtype, pin_memory=True)  # noqa: E731
+        self.hin = []
         for p in self.precs:
-            for key in ("pd", "p4"):
-                st = t.cuda.Stream()
-                p[key].set_stream(st.cuda_stream)
-                p[key].set_host_async(True)
-                self.e2e_plans.append((p[key], st))
-        h2d = d2h = 0
-        for p in self.precs:
-            pin = lambda x: t.empty(x.shape, dtype=x.dtype, pin_memory=True)  # noqa: E731
-            h = dict(x=pin(p["xs"][0]), y=pin(p["y"]), r=pin(p["rs"][0]), c=pin(p["c"]), s=pin(p["s"]))
+            h = dict(x=pin(p["xs"][0]), r=pin(p["rs"][0]))
             h["x"].copy_(p["xs"][0].cpu())
             h["r"].copy_(p["rs"][0].cpu())
-            self.host.append(h)
-            h2d += h["x"].numel() * h["x"].element_size() + 2 * h["r"].numel() * h["r"].element_size()
+            self.hin.append(h)
+        self.e2e_sets = []
+        for k in range(2):
+            plans, host = [], []
+            for p in self.precs:
+                pd = p["pd"] if k == 0 else p["eng"].plan("dft", (self.n_dft,))
+                p4 = p["p4"] if k == 0 else p["eng"].plan("t4", (self.n_t4,))
+                streams = []
+                for plan in (pd, p4):
+                    st = t.cuda.Stream()
+                    plan.set_stream(st.cuda_stream)
+                    plan.set_host_async(True)
+                    streams.append(st)
+                plans.append((pd, p4, streams))
+                host.append(dict(y=pin(p["y"]), c=pin(p["c"]), s=pin(p["s"])))
+            self.e2e_sets.append((plans, host))
+        self.e2e_k = 0
+        h2d = d2h = 0
+        for hi, h in zip(self.hin, self.e2e_sets[0][1]):
+            h2d += hi["x"].numel() * hi["x"].element_size() + 2 * hi["r"].numel() * hi["r"].element_size()
             d2h += h["y"].numel() * h["y"].element_size() + 2 * h["c"].numel() * h["c"].element_size()
         return h2d, d2h
 
     def e2e_step(self):
-        for p, h in zip(self.precs, self.host):
-            p["pd"]("dft", h["x"].data_ptr(), h["y"].data_ptr(), check=False)
-            p["p4"]("dct4", h["r"].data_ptr(), h["c"].data_ptr(), check=False)
-            p["p4"]("dst4", h["r"].data_ptr(), h["s"].data_ptr(), check=False)
-        for plan, _ in self.e2e_plans:
-            plan.synchronize()
+        plans, host = self.e2e_sets[self.e2e_k & 1]
+        if self.e2e_k >= 2:
+            for pd, p4, _ in plans:
+                pd.synchronize()
+                p4.synchronize()
+        self.e2e_k += 1
+        for (pd, p4, _), hi, h in zip(plans, self.hin, host):
+            pd("dft", hi["x"].data_ptr(), h["y"].data_ptr(), check=False)
+            p4("dct4", hi["r"].data_ptr(), h["c"].data_ptr(), check=False)
+            p4("dst4", hi["r"].data_ptr(), h["s"].data_ptr(), check=False)
 
     def config(self):
         return {"workload": "1-D dft 2^26 (c128, c64) + dct4/dst4 2^24 (f64, f32)",
