@@ -281,6 +281,47 @@ __device__ __forceinline__ void row_s2g(real* g, const real* sr, int j) {
 __device__ __forceinline__ bool rows_staged_in(const AxisParams& p) { return !p.colmode && p.in_n == 1; }
 __device__ __forceinline__ bool rows_staged_out(const AxisParams& p) { return !p.colmode && p.out_k == 1; }
 
+// ------------------------------------------------------- HBM pre-twiddle
+// In a pass of a Stockham FFT over HBM, element n of a sub-DFT with span
+// index q is multiplied by w_Lt^g, g = q*n*Lt/(st_ns*L), each root read as
+// the product of a coarse and a fine table entry.  Thread j holds
+// n = j + r*TPT, so its roots are w^g0 * d^r with w^g0 = w_Lt^(q*j*s) and
+// d = w_Lt^(q*TPT*s) (s = 2^st_shift): three table roots per thread (w^g0,
+// d, d^4), the other powers of d formed as at most two products, as the
+// in-CTA passes form theirs (apply_root_powers).
+template <int L, int R>
+__device__ __forceinline__ void hbm_pretwiddle(cpx (&v)[R], const AxisParams& p, int64_t b0, int j) {
+  constexpr int TPT = L / R;
+  const int64_t q = (b0 / p.st_div) & (p.st_ns - 1);
+  const int64_t lomask = (int64_t(1) << p.st_lobits) - 1;
+  auto root = [&](int64_t g) { return cmul(ldg(p.st_hi + (g >> p.st_lobits)), ldg(p.st_lo + (g & lomask))); };
+  if constexpr (R < 4) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = cmul(v[r], root((q * (j + r * TPT)) << p.st_shift));
+  } else {
+    const int64_t gd = (q * TPT) << p.st_shift;
+    const cpx base = root((q * j) << p.st_shift);
+    const cpx d1 = root(gd);
+    const cpx d2 = cmul(d1, d1);
+    const cpx d3 = cmul(d2, d1);
+    const cpx d4 = R > 4 ? root(4 * gd) : czero();
+    const cpx d8 = cmul(d4, d4);
+    const cpx d12 = cmul(d8, d4);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int lo = r & 3, hi = r >> 2;
+      cpx w = base;
+      if (hi == 1) w = cmul(w, d4);
+      if (hi == 2) w = cmul(w, d8);
+      if (hi == 3) w = cmul(w, d12);
+      if (lo == 1) w = cmul(w, d1);
+      if (lo == 2) w = cmul(w, d2);
+      if (lo == 3) w = cmul(w, d3);
+      v[r] = cmul(v[r], w);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- load ops
 // Each load op fills v[r] with complex input element n = j + r*(L/R) of the
 // length-L DFT of transform x.b.
@@ -309,19 +350,7 @@ struct LoadCplx {
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r].y = -v[r].y;
     }
-    if (p.st_ns > 1) {
-      // element n of span index q is multiplied by w_Lt^(q*n*Lt/(st_ns*L)),
-      // read as the product of a coarse and a fine table entry
-      const int64_t q = (x.b0 / p.st_div) & (p.st_ns - 1);
-      const int64_t lomask = (int64_t(1) << p.st_lobits) - 1;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int64_t n = x.j + r * (L / R);
-        const int64_t g = (q * n) << p.st_shift;
-        const cpx w = cmul(ldg(p.st_hi + (g >> p.st_lobits)), ldg(p.st_lo + (g & lomask)));
-        v[r] = cmul(v[r], w);
-      }
-    }
+    if (p.st_ns > 1) hbm_pretwiddle<L, R>(v, p, x.b0, x.j);
   }
 };
 

@@ -80,16 +80,7 @@ struct PCplx {
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r].y = -v[r].y;
     }
-    if (p.st_ns > 1) {
-      const int64_t q = (x.b0 / p.st_div) & (p.st_ns - 1);
-      const int64_t lomask = (int64_t(1) << p.st_lobits) - 1;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int64_t n = x.j + r * (L / R);
-        const int64_t g = (q * n) << p.st_shift;
-        v[r] = cmul(v[r], cmul(ldg(p.st_hi + (g >> p.st_lobits)), ldg(p.st_lo + (g & lomask))));
-      }
-    }
+    if (p.st_ns > 1) hbm_pretwiddle<L, R>(v, p, x.b0, x.j);
   }
 };
 
