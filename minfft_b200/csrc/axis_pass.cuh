@@ -526,6 +526,11 @@ struct LoadDCT3 {
   // z_n of the type-3 pre-rotation; rd(i) returns input real x_i
   template <class Rd>
   static __device__ __forceinline__ cpx zval_r(const Rd& rd, int n, int L, bool dst, const cpx* e) {
+    return zval_w(rd, n, L, dst, [&](int m) { return ldg(e + m); });
+  }
+  // z_n with the root w_4N^n from a function
+  template <class Rd, class Rt>
+  static __device__ __forceinline__ cpx zval_w(const Rd& rd, int n, int L, bool dst, const Rt& root) {
     const int N = 2 * L;
     if (n == 0) return cmk(dst ? rd(N - 1) : rd(0), real(0));
     if (n == L) {
@@ -534,7 +539,7 @@ struct LoadDCT3 {
     }
     const real a = dst ? rd(N - n - 1) : rd(n);
     const real b = dst ? rd(n - 1) : rd(N - n);
-    return cconj(cmul(cmk(a, b), ldg(e + n)));
+    return cconj(cmul(cmk(a, b), root(n)));
   }
   static __device__ __forceinline__ cpx zval(const real* in, int64_t s, int n, int L, bool dst, const cpx* e) {
     return zval_r([&](int i) { return in[int64_t(i) * s]; }, n, L, dst, e);

@@ -15,6 +15,15 @@ struct LineParams {
   int64_t in_so, in_sn, out_so, out_sn;
   const cpx* t1;
   const cpx* t2;
+  // optional coarse/fine form of t1 and t2 for long lines: entry i of table
+  // k is the root w^e, e = mul_k*i + add_k, read as hi_k[e >> bits_k] *
+  // lo_k[e & (2^bits_k - 1)] instead of a table of the full line length
+  const cpx* hi1;
+  const cpx* lo1;
+  const cpx* hi2;
+  const cpx* lo2;
+  int bits1, mul1, add1;
+  int bits2, mul2, add2;
   int flags;
   int mode;
   real scale;

@@ -16,6 +16,17 @@
 
 namespace mb {
 
+// Entry i of the kind tables t1 / t2 (coarse/fine product when given).
+__device__ __forceinline__ cpx cf_root(const cpx* hi, const cpx* lo, int bits, int64_t e) {
+  return cmul(ldg(hi + (e >> bits)), ldg(lo + (e & ((int64_t(1) << bits) - 1))));
+}
+__device__ __forceinline__ cpx root1(const LineParams& p, int64_t i) {
+  return p.hi1 ? cf_root(p.hi1, p.lo1, p.bits1, i * p.mul1 + p.add1) : ldg(p.t1 + i);
+}
+__device__ __forceinline__ cpx root2(const LineParams& p, int64_t i) {
+  return p.hi2 ? cf_root(p.hi2, p.lo2, p.bits2, i * p.mul2 + p.add2) : ldg(p.t2 + i);
+}
+
 struct ItemIdx {
   int64_t o, n, i;
 };
@@ -62,7 +73,7 @@ struct Op_t4_pre {
     const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
     const real a = in[(2 * it.n) * p.in_sn];
     const real b = in[(N - 1 - 2 * it.n) * p.in_sn];
-    const cpx w = ldg(p.t1 + it.n);
+    const cpx w = root1(p, it.n);
     cpx v;
     if (!dst) {
       v = cmul(w, cmk(a, b));
@@ -93,7 +104,7 @@ struct Op_c2r_pack {
       out[k * p.out_sn] = cmk(2 * z0.x, 2 * z0.y);
     } else {
       cpx ta, tb;
-      pack_pair(z0, z1, ldg(p.t2 + k), ta, tb);
+      pack_pair(z0, z1, root2(p, k), ta, tb);
       out[k * p.out_sn] = cconj(ta);
       out[(L - k) * p.out_sn] = cconj(tb);
     }
@@ -114,15 +125,16 @@ struct Op_dct3_pack {
     const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
     cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
     const int k = int(it.n);
-    const cpx z0 = LoadDCT3::zval(in, p.in_sn, k, int(L), dst, p.t1);
-    const cpx z1 = LoadDCT3::zval(in, p.in_sn, int(L) - k, int(L), dst, p.t1);
+    auto rd = [&](int i) { return in[int64_t(i) * p.in_sn]; };
+    const cpx z0 = LoadDCT3::zval_w(rd, k, int(L), dst, [&](int n) { return root1(p, n); });
+    const cpx z1 = LoadDCT3::zval_w(rd, int(L) - k, int(L), dst, [&](int n) { return root1(p, n); });
     if (k == 0) {
       out[0] = cmk(z0.x + z1.x, -(z0.x - z1.x));
     } else if (2 * k == L) {
       out[k * p.out_sn] = cmk(2 * z0.x, 2 * z0.y);
     } else {
       cpx ta, tb;
-      pack_pair(z0, z1, ldg(p.t2 + k), ta, tb);
+      pack_pair(z0, z1, root2(p, k), ta, tb);
       out[k * p.out_sn] = cconj(ta);
       out[(L - k) * p.out_sn] = cconj(tb);
     }
@@ -149,7 +161,7 @@ struct Op_r2c_unpack {
       out[k * p.out_sn] = cconj(za);
     } else {
       cpx xa, xb;
-      unpack_pair(za, in[(L - k) * p.in_sn], ldg(p.t1 + k), xa, xb);
+      unpack_pair(za, in[(L - k) * p.in_sn], root1(p, k), xa, xb);
       out[k * p.out_sn] = xa;
       out[(L - k) * p.out_sn] = xb;
     }
@@ -180,12 +192,12 @@ struct Op_dct2_post {
       out[int64_t(dst ? N - 1 : 0) * p.out_sn] = 2 * v0;
       out[int64_t(dst ? L - 1 : L) * p.out_sn] = r2 * vl;
     } else if (2 * k == L) {
-      StoreDCT2::emit(out, p.out_sn, k, N, dst, cconj(za), ldg(p.t1 + k));
+      StoreDCT2::emit(out, p.out_sn, k, N, dst, cconj(za), root1(p, k));
     } else {
       cpx xa, xb;
-      unpack_pair(za, in[(L - k) * p.in_sn], ldg(p.t2 + k), xa, xb);
-      StoreDCT2::emit(out, p.out_sn, k, N, dst, xa, ldg(p.t1 + k));
-      StoreDCT2::emit(out, p.out_sn, int(L) - k, N, dst, xb, ldg(p.t1 + (L - k)));
+      unpack_pair(za, in[(L - k) * p.in_sn], root2(p, k), xa, xb);
+      StoreDCT2::emit(out, p.out_sn, k, N, dst, xa, root1(p, k));
+      StoreDCT2::emit(out, p.out_sn, int(L) - k, N, dst, xb, root1(p, L - k));
     }
   }
 };
@@ -225,8 +237,8 @@ struct Op_t4_post {
     const cpx T = static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i];
     real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
     const int64_t m = it.n;
-    const cpx a = cmul(ldg(p.t2 + 2 * m), T);
-    const cpx b = cmul(ldg(p.t2 + (N - 1 - 2 * m)), cconj(T));
+    const cpx a = cmul(root2(p, 2 * m), T);
+    const cpx b = cmul(root2(p, N - 1 - 2 * m), cconj(T));
     out[(2 * m) * p.out_sn] = 2 * (dst ? a.y : a.x);
     out[(N - 1 - 2 * m) * p.out_sn] = 2 * (dst ? b.y : b.x);
   }

@@ -819,6 +819,28 @@ struct Planner {
     }
   }
 
+  // roots w_M^(mul*i + add) of a long line's pre/post step as the product of
+  // a coarse and a fine table (slot 1 replaces lp.t1, slot 2 lp.t2): two
+  // tables of about sqrt(M) entries instead of one of the line's length
+  void set_root_pair(LineParams& lp, int slot, int64_t M, int mul, int add) {
+    const cpx* hi = tab(TB_STHI, M);
+    const cpx* lo = tab(TB_STLO, M);
+    const int bits = (int)st_lobits_for(M);
+    if (slot == 1) {
+      lp.hi1 = hi;
+      lp.lo1 = lo;
+      lp.bits1 = bits;
+      lp.mul1 = mul;
+      lp.add1 = add;
+    } else {
+      lp.hi2 = hi;
+      lp.lo2 = lo;
+      lp.bits2 = bits;
+      lp.mul2 = mul;
+      lp.add2 = add;
+    }
+  }
+
   int pick_temp(std::initializer_list<int> exclude) {
     for (int b : {BUF_T2, BUF_T3, BUF_T4}) {
       bool bad = false;
@@ -910,15 +932,15 @@ struct Planner {
         which = mb::LK_DCT2_PRE;
       } else if (s.combo == mb::K_T4) {
         which = mb::LK_T4_PRE;
-        lp.t1 = tab(TB_T4PRE, s.N);
+        set_root_pair(lp, 1, 2 * s.N, 1, 0);  // w_2N^n
       } else if (s.combo == mb::K_C2R) {
         which = mb::LK_C2R_PACK;
-        lp.t2 = tab(TB_RFT, s.N);
+        set_root_pair(lp, 2, s.N, 1, 0);  // w_N^k
         items = outer * inner * (Lt / 2 + 1);
       } else {
         which = mb::LK_DCT3_PACK;
-        lp.t1 = tab(TB_T23, s.N);
-        lp.t2 = tab(TB_RFT, s.N);
+        set_root_pair(lp, 1, 4 * s.N, 1, 0);  // w_4N^n
+        set_root_pair(lp, 2, s.N, 1, 0);      // w_N^k
         items = outer * inner * (Lt / 2 + 1);
       }
       add_line_kernel(which, lp, items, s.in_buf, cs);
@@ -986,17 +1008,17 @@ struct Planner {
       int64_t items = outer * inner * (Lt / 2 + 1);
       if (s.combo == mb::K_R2C) {
         which = mb::LK_R2C_UNPACK;
-        lp.t1 = tab(TB_RFT, s.N);
+        set_root_pair(lp, 1, s.N, 1, 0);  // w_N^k
       } else if (s.combo == mb::K_DCT2) {
         which = mb::LK_DCT2_POST;
-        lp.t1 = tab(TB_T23, s.N);
-        lp.t2 = tab(TB_RFT, s.N);
+        set_root_pair(lp, 1, 4 * s.N, 1, 0);  // w_4N^n
+        set_root_pair(lp, 2, s.N, 1, 0);      // w_N^k
       } else if (s.combo == mb::K_DCT3) {
         which = mb::LK_DCT3_POST;
         items = outer * inner * Lt;
       } else {
         which = mb::LK_T4_POST;
-        lp.t2 = tab(TB_T4POST, s.N);
+        set_root_pair(lp, 2, 8 * s.N, 2, 1);  // w_8N^(2q+1)
         items = outer * inner * Lt;
       }
       add_line_kernel(which, lp, items, cd, s.out_buf);
