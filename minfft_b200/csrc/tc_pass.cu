@@ -16,9 +16,10 @@
 // [[C, S], [-S, C]] (C = cos, S = sin of 2*pi*k*n/16) acting on
 // (Re x, Im x), so a stage is D[128 x 32] = A[128 x 32] * B^T with A the
 // sub-DFT inputs (K-major, one row per sub-DFT) and B the fixed matrix.
-// Tensor cores take FP16 or BF16 operands; to keep FP32 accuracy every row
-// of A is scaled by its own power of two (bringing its largest component to
-// [256, 512)) and split into 16-bit terms, as is B:
+// Tensor cores take FP16 or BF16 operands; to keep FP32 accuracy each
+// transform is scaled by a power of two (bringing the largest component of
+// its input to [256, 512); the scale is undone when the result is stored)
+// and every row of A is split into 16-bit terms, as is B:
 //   FP16: A = A0 + A1, B = B0 + B1 (11 + 11 significant bits), D = A0 B0 +
 //         A0 B1 + A1 B0                                  (3 products)
 //   BF16: A = A0 + A1 + A2 (8 + 8 + 8 bits), likewise B; the six products
@@ -109,7 +110,8 @@ struct TcLayout {
   static constexpr int b_off = region;
   static constexpr int offs_off = b_off + NT * kBBytes;
   static constexpr int mbar_off = offs_off + 4 * TB * 8;  // two sets of tile offsets
-  static constexpr int total = mbar_off + 16;
+  static constexpr int inv_off = mbar_off + 16;  // per-transform unscale factors
+  static constexpr int total = inv_off + (TB * 4 + 15) / 16 * 16;
   static constexpr int tmem_cols = 64 * G;  // per group: leading accumulator, correction accumulator
   static_assert(tmem_cols == 64 * (TB / 8), "tc_tmem_columns");
 };
@@ -236,6 +238,7 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + Lay::mbar_off);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + Lay::mbar_off + 8);
   int* bad = reinterpret_cast<int*>(sm + Lay::mbar_off + 12);
+  float* invs = reinterpret_cast<float*>(sm + Lay::inv_off);
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
@@ -304,7 +307,7 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
     // ---- the next tile's loads are issued now and land during the stages
     if (next < ntiles) load_tile<TB>(p, nxt, valid(next), tid, v);
 
-#pragma unroll 1
+#pragma unroll
     for (int stage = 0; stage < 2; ++stage) {
       // ---- this row's inputs: stage 1 x[16*n1 + n2], stage 2 y[16*k1 + n2]
       float re[16], im[16];
@@ -315,13 +318,22 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
         re[i] = u.x;
         im[i] = u.y;
       }
-      float mx = 0.f;
+      // one scale 2^s per transform, from its input: the largest input
+      // component goes to [2^8, 2^9); the stage-1 outputs stay scaled (at most
+      // 16*sqrt(2)*2^9 < 2^14 in magnitude, inside the FP16 range) and the
+      // store unscales
+      float sc = 1.f;
+      if (stage == 0) {
+        float mx = 0.f;
 #pragma unroll
-      for (int i = 0; i < 16; ++i) mx = fmaxf(mx, fmaxf(fabsf(re[i]), fabsf(im[i])));
-      // row scale 2^s with the largest component scaled into [2^8, 2^9)
-      const int ex = (__float_as_int(mx) >> 23) & 0xFF;  // biased exponent (mx >= 0)
-      const int s = min(max(135 - ex, -126), 126);
-      const float sc = pow2i(s), inv = pow2i(-s);
+        for (int i = 0; i < 16; ++i) mx = fmaxf(mx, fmaxf(fabsf(re[i]), fabsf(im[i])));
+#pragma unroll
+        for (int o = 8; o >= 1; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));  // the 16 rows
+        const int ex = (__float_as_int(mx) >> 23) & 0xFF;  // biased exponent (mx >= 0)
+        const int s = min(max(135 - ex, -126), 126);
+        sc = pow2i(s);
+        if (dgt == 0) invs[t] = pow2i(-s);
+      }
       __syncthreads();  // the tile is read: the A operands overwrite it
       // ---- split into NT terms and write the A operands (K: Re 0..15, Im 16..31)
 #pragma unroll
@@ -331,7 +343,11 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
         for (int u = 0; u < 8; u += 2) {
           uint32_t o[3];
           const int k = kb * 8 + u;
-          split_pair<FMT, NT>((k < 16 ? re[k] : im[k - 16]) * sc, (k + 1 < 16 ? re[k + 1] : im[k + 1 - 16]) * sc, o);
+          const float a = k < 16 ? re[k] : im[k - 16], b = k + 1 < 16 ? re[k + 1] : im[k + 1 - 16];
+          if (stage == 0)
+            split_pair<FMT, NT>(a * sc, b * sc, o);
+          else
+            split_pair<FMT, NT>(a, b, o);
 #pragma unroll
           for (int z = 0; z < NT; ++z) w[z][u / 2] = o[z];
         }
@@ -391,12 +407,12 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
         tmem_ld16(taddr + 32, e);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int k = 0; k < 16; ++k) re[k] = (__uint_as_float(d[k]) + __uint_as_float(e[k])) * inv;
+        for (int k = 0; k < 16; ++k) re[k] = __uint_as_float(d[k]) + __uint_as_float(e[k]);
         tmem_ld16(taddr + 16, d);
         tmem_ld16(taddr + 48, e);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int k = 0; k < 16; ++k) im[k] = (__uint_as_float(d[k]) + __uint_as_float(e[k])) * inv;
+        for (int k = 0; k < 16; ++k) im[k] = __uint_as_float(d[k]) + __uint_as_float(e[k]);
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       // the MMAs have completed (mbarrier), so the A region is free again
@@ -424,7 +440,7 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
         const int c = p.colmode ? (e % TB) : (e / kL);
         const int n = p.colmode ? (e / TB) : (e % kL);
         if (c < nv) {
-          cpx x = data[c * kLP + pad16(n)];
+          cpx x = cscale(data[c * kLP + pad16(n)], invs[c]);
           if (cj_out) x.y = -x.y;
           out[cur[TB + c] + int64_t(n) * p.out_k] = x;
         }
