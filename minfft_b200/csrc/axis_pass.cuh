@@ -21,11 +21,38 @@
 // through padded shared memory.  The last pass leaves output element
 // k = j + r*(L/R) in register r, so the first load and the last store need
 // no shared memory at all for the plain complex transform.
+//
+// Kind roots.  The load and store stages multiply by roots w_M^k of the kind
+// tables at k = j + i*(L/R).  Thread j reads only table entry j (one load per
+// table) and forms the others as w_M^j * w_M^(i*L/R); for the tables used
+// here M is 2L, 4L or 8L, so the second factor is the 128th root of unity
+// w_128^(i*128L/(M*R)), a constant-memory operand (w128).  When L/R = 1 the
+// only thread is j = 0 and w_M^0 = 1 is not read at all.
 #pragma once
 
 #include "common.cuh"
+#include "roots128.h"
 
 namespace mb {
+
+// w_128^m, m < 32 (m is a compile-time constant once the caller's loop is unrolled)
+__device__ __forceinline__ cpx w128(int m) {
+#if MINFFT_SINGLE
+  return cmk(roots128::kReF[m], roots128::kImF[m]);
+#else
+  return cmk(roots128::kReD[m], roots128::kImD[m]);
+#endif
+}
+
+// Entry j of a kind table: the base of this thread's roots (see above).
+template <int TPT>
+__device__ __forceinline__ cpx kind_base(const cpx* table, int j) {
+  if constexpr (TPT == 1) {
+    return cmk(real(1), real(0));
+  } else {
+    return ldg(table + j);
+  }
+}
 
 struct AxisParams {
   const void* in;
@@ -433,12 +460,12 @@ struct LoadT4 {
     const real* lo = in + int64_t(2 * x.j) * s;
     const real* hi = in + int64_t(N - 1 - 2 * x.j) * s;
     const int64_t st = int64_t(2 * TPT) * s;
-    const cpx* e = p.t1 + x.j;
+    const cpx e = kind_base<TPT>(p.t1, x.j);  // w_2N^j; w_2N^(j + r*TPT) = e * w_4R^r
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const real a = lo[r * st];
       const real b = hi[-r * st];
-      const cpx w = ldg(e + r * TPT);
+      const cpx w = cmul(e, w128(r * (32 / R)));
       if (!dst) {
         v[r] = cmul(w, cmk(a, b));
       } else {
@@ -475,8 +502,8 @@ __device__ __forceinline__ void unpack_pair(cpx za, cpx zb, cpx f, cpx& xa, cpx&
 // Visits the spectrum pairs (k, L-k), k = 0 .. L/2, owned by thread j of a
 // transform: k = j + i*TPT for i = 0 .. R/2 (only j = 0 reaches k = L/2).
 // zf(k) reads a spectrum value -- for k = 0 also zf(L), which readers of an
-// L-element tile must fold back into range; body(k, z_k, z_{L-k}) consumes
-// the pair.
+// L-element tile must fold back into range; body(i, k, z_k, z_{L-k})
+// consumes the pair.
 template <int L, int R, class Zf, class Body>
 __device__ __forceinline__ void pair_loop(const Ctx& x, const Zf& zf, const Body& body) {
   constexpr int TPT = L / R;
@@ -484,20 +511,35 @@ __device__ __forceinline__ void pair_loop(const Ctx& x, const Zf& zf, const Body
   for (int i = 0; i <= R / 2; ++i) {
     const int k = x.j + i * TPT;
     if (i == R / 2 && x.j != 0) break;
-    body(k, zf(k), zf(L - k));
+    body(i, k, zf(k), zf(L - k));
   }
 }
 
+// w_N^k (N = 2L) at k = j + i*(L/R) from base = w_N^j (kind roots, above);
+// used for 0 < k < L/2, i.e. i < R/2 (other i map to w_128^0 and stay
+// inside the constant table).
+template <int R>
+__device__ __forceinline__ cpx rft_root(cpx base, int i) {
+  return cmul(base, w128((i < R / 2 ? i : 0) * (64 / R)));
+}
+// w_4N^k (N = 2L) at k = j + i*(L/R) from base = w_4N^j.
+template <int R>
+__device__ __forceinline__ cpx t23_root(cpx base, int i) {
+  return cmul(base, w128(i * (16 / R)));
+}
+// w_4N^(L-k) from w_4N^k: w_4N^L = w_8 times the conjugate.
+__device__ __forceinline__ cpx t23_mirror(cpx rk) { return cmulc(w128(16), rk); }
+
 // Packs the pair (z_k, z_{L-k}) into the conjugated inverse-DFT inputs t_k,
-// t_{L-k} of the tile (k = 0 and k = L/2 are the self-paired ends).
-__device__ __forceinline__ void pack_into(const Tile& t, int c, int k, int L, cpx z0, cpx z1, const cpx* f) {
+// t_{L-k} of the tile (k = 0 and k = L/2 are the self-paired ends); f = w_N^k.
+__device__ __forceinline__ void pack_into(const Tile& t, int c, int k, int L, cpx z0, cpx z1, cpx f) {
   if (k == 0) {
     t.s[t.idx(c, 0)] = cmk(z0.x + z1.x, -(z0.x - z1.x));
   } else if (2 * k == L) {
     t.s[t.idx(c, k)] = cmk(2 * z0.x, 2 * z0.y);
   } else {
     cpx ta, tb;
-    pack_pair(z0, z1, ldg(f + k), ta, tb);
+    pack_pair(z0, z1, f, ta, tb);
     t.s[t.idx(c, k)] = cconj(ta);
     t.s[t.idx(c, L - k)] = cconj(tb);
   }
@@ -511,8 +553,9 @@ struct LoadC2R {
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
     const cpx* in = static_cast<const cpx*>(p.in) + x.oin;
+    const cpx b2 = kind_base<L / R>(p.t2, x.j);
     pair_loop<L, R>(x, [&](int k) { return x.active ? in[int64_t(k) * p.in_n] : czero(); },
-                    [&](int k, cpx z0, cpx z1) { pack_into(t, x.c, k, L, z0, z1, p.t2); });
+                    [&](int i, int k, cpx z0, cpx z1) { pack_into(t, x.c, k, L, z0, z1, rft_root<R>(b2, i)); });
     __syncthreads();
     gather_natural<L, R>(v, x.j, x.c, t);
   }
@@ -552,30 +595,44 @@ struct LoadDCT3 {
       if (rows_staged_in(p)) {
         // the row through shared memory; every thread reads its pairs before
         // any packed value overwrites the row
+        constexpr int TPT = L / R;
+        const cpx b1 = kind_base<TPT>(p.t1, x.j), b2 = kind_base<TPT>(p.t2, x.j);
         real* sr = tile_row(t, x.c);
         if (x.active) row_g2s<L, R>(sr, in, x.j);
         __syncthreads();
-        constexpr int TPT = L / R;
         constexpr int NP = R / 2 + 1;
         cpx za[NP], zb[NP];
+        auto rd = [&](int m) { return sr[m]; };
 #pragma unroll
         for (int i = 0; i < NP; ++i) {
           const int k = x.j + i * TPT;
           const bool own = x.active && (i < R / 2 || x.j == 0);
-          za[i] = own ? zval(sr, 1, k, L, dst, p.t1) : czero();
-          zb[i] = own ? zval(sr, 1, L - k, L, dst, p.t1) : czero();
+          const cpx rk = t23_root<R>(b1, i);  // w_4N^k
+          za[i] = own ? zval_w(rd, k, L, dst, [&](int) { return rk; }) : czero();
+          zb[i] = own ? zval_w(rd, L - k, L, dst, [&](int) { return t23_mirror(rk); }) : czero();
         }
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < NP; ++i)
-          if (i < R / 2 || x.j == 0) pack_into(t, x.c, x.j + i * TPT, L, za[i], zb[i], p.t2);
+          if (i < R / 2 || x.j == 0) pack_into(t, x.c, x.j + i * TPT, L, za[i], zb[i], rft_root<R>(b2, i));
         __syncthreads();
         gather_natural<L, R>(v, x.j, x.c, t);
         return;
       }
     }
-    pair_loop<L, R>(x, [&](int k) { return x.active ? zval(in, p.in_n, k, L, dst, p.t1) : czero(); },
-                    [&](int k, cpx z0, cpx z1) { pack_into(t, x.c, k, L, z0, z1, p.t2); });
+    // the pairs (k, L-k) of pair_loop, read straight from global memory
+    constexpr int TPT = L / R;
+    const cpx b1 = kind_base<TPT>(p.t1, x.j), b2 = kind_base<TPT>(p.t2, x.j);
+    auto rd = [&](int m) { return in[int64_t(m) * p.in_n]; };
+#pragma unroll
+    for (int i = 0; i <= R / 2; ++i) {
+      const int k = x.j + i * TPT;
+      if (i == R / 2 && x.j != 0) break;
+      const cpx rk = t23_root<R>(b1, i);  // w_4N^k
+      const cpx z0 = x.active ? zval_w(rd, k, L, dst, [&](int) { return rk; }) : czero();
+      const cpx z1 = x.active ? zval_w(rd, L - k, L, dst, [&](int) { return t23_mirror(rk); }) : czero();
+      pack_into(t, x.c, k, L, z0, z1, rft_root<R>(b2, i));
+    }
     __syncthreads();
     gather_natural<L, R>(v, x.j, x.c, t);
   }
@@ -643,7 +700,8 @@ struct StoreR2C {
     __syncthreads();
     if (!x.active) return;
     cpx* out = static_cast<cpx*>(p.out) + x.oout;
-    pair_loop<L, R>(x, [&](int k) { return t.s[t.idx(x.c, k & (L - 1))]; }, [&](int k, cpx za, cpx zb) {
+    const cpx b1 = kind_base<L / R>(p.t1, x.j);
+    pair_loop<L, R>(x, [&](int k) { return t.s[t.idx(x.c, k & (L - 1))]; }, [&](int i, int k, cpx za, cpx zb) {
       if (k == 0) {
         out[0] = cmk(za.x + za.y, real(0));
         out[int64_t(L) * p.out_k] = cmk(za.x - za.y, real(0));
@@ -651,7 +709,7 @@ struct StoreR2C {
         out[int64_t(k) * p.out_k] = cconj(za);
       } else {
         cpx xa, xb;
-        unpack_pair(za, zb, ldg(p.t1 + k), xa, xb);
+        unpack_pair(za, zb, rft_root<R>(b1, i), xa, xb);
         out[int64_t(k) * p.out_k] = xa;
         out[int64_t(L - k) * p.out_k] = xb;
       }
@@ -684,18 +742,20 @@ struct StoreDCT2 {
     const bool dst = (p.flags & F_DST) != 0;
     constexpr int N = 2 * L;
     const real r2 = real(1.414213562373095048801688724209698079);
-    pair_loop<L, R>(x, [&](int k) { return t.s[t.idx(x.c, k & (L - 1))]; }, [&](int k, cpx za, cpx zb) {
+    const cpx b1 = kind_base<L / R>(p.t1, x.j), b2 = kind_base<L / R>(p.t2, x.j);
+    pair_loop<L, R>(x, [&](int k) { return t.s[t.idx(x.c, k & (L - 1))]; }, [&](int i, int k, cpx za, cpx zb) {
       if (k == 0) {
         const real v0 = za.x + za.y, vl = za.x - za.y;
         out[int64_t(dst ? N - 1 : 0) * p.out_k] = 2 * v0;
         out[int64_t(dst ? L - 1 : L) * p.out_k] = r2 * vl;
       } else if (2 * k == L) {
-        emit(out, p.out_k, k, N, dst, cconj(za), ldg(p.t1 + k));
+        emit(out, p.out_k, k, N, dst, cconj(za), w128(8));  // w_4N^(L/2) = w_16
       } else {
         cpx xa, xb;
-        unpack_pair(za, zb, ldg(p.t2 + k), xa, xb);
-        emit(out, p.out_k, k, N, dst, xa, ldg(p.t1 + k));
-        emit(out, p.out_k, L - k, N, dst, xb, ldg(p.t1 + L - k));
+        unpack_pair(za, zb, rft_root<R>(b2, i), xa, xb);
+        const cpx e = t23_root<R>(b1, i);  // w_4N^k
+        emit(out, p.out_k, k, N, dst, xa, e);
+        emit(out, p.out_k, L - k, N, dst, xb, t23_mirror(e));
       }
     });
   }
@@ -796,13 +856,15 @@ struct StoreT4 {
     real* lo = out + int64_t(2 * x.j) * s;
     real* hi = out + int64_t(N - 1 - 2 * x.j) * s;
     const int64_t st = int64_t(2 * TPT) * s;
-    const cpx* glo = p.t2 + 2 * x.j;
-    const cpx* ghi = p.t2 + (N - 1 - 2 * x.j);
+    // t2[q] = w_8N^(2q+1): t2[2m] = t2[2j] * w_4R^r and t2[N-1-2m] =
+    // t2[N-1-2j] * conj(w_4R^r) for m = j + r*TPT
+    const cpx glo = ldg(p.t2 + 2 * x.j);
+    const cpx ghi = ldg(p.t2 + (N - 1 - 2 * x.j));
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const cpx T = v[r];
-      const cpx a = cmul(ldg(glo + 2 * r * TPT), T);
-      const cpx b = cmul(ldg(ghi - 2 * r * TPT), cconj(T));
+      const cpx a = cmul(cmul(glo, w128(r * (32 / R))), T);
+      const cpx b = cmul(cmulc(ghi, w128(r * (32 / R))), cconj(T));
       lo[r * st] = 2 * (dst ? a.y : a.x);
       hi[-r * st] = 2 * (dst ? b.y : b.x);
     }
