@@ -304,6 +304,20 @@ __device__ __forceinline__ void row_s2g(real* g, const real* sr, int j) {
   }
 }
 
+// Column mode: thread j of the transform moves reals n = j + m*TPT (m < 2R)
+// of its column (element stride s) into the column's tile slot, all loads
+// issued before any store; a warp's load covers cpb adjacent columns of a
+// few rows.
+template <int L, int R>
+__device__ __forceinline__ void col_g2s(real* sr, const real* g, int64_t s, int j) {
+  constexpr int TPT = L / R;
+  real r[2 * R];
+#pragma unroll
+  for (int m = 0; m < 2 * R; ++m) r[m] = __ldcs(g + int64_t(j + m * TPT) * s);
+#pragma unroll
+  for (int m = 0; m < 2 * R; ++m) sr[j + m * TPT] = r[m];
+}
+
 // row mode with unit element strides
 __device__ __forceinline__ bool rows_staged_in(const AxisParams& p) { return !p.colmode && p.in_n == 1; }
 __device__ __forceinline__ bool rows_staged_out(const AxisParams& p) { return !p.colmode && p.out_k == 1; }
@@ -592,13 +606,19 @@ struct LoadDCT3 {
     const real* in = static_cast<const real*>(p.in) + x.oin;
     const bool dst = (p.flags & F_DST) != 0;
     if constexpr (L >= 2) {
-      if (rows_staged_in(p)) {
-        // the row through shared memory; every thread reads its pairs before
-        // any packed value overwrites the row
+      if (rows_staged_in(p) || p.colmode) {
+        // the row (or column) through shared memory, its loads all issued
+        // up front; every thread reads its pairs before any packed value
+        // overwrites the row
         constexpr int TPT = L / R;
         const cpx b1 = kind_base<TPT>(p.t1, x.j), b2 = kind_base<TPT>(p.t2, x.j);
         real* sr = tile_row(t, x.c);
-        if (x.active) row_g2s<L, R>(sr, in, x.j);
+        if (x.active) {
+          if (p.colmode)
+            col_g2s<L, R>(sr, in, p.in_n, x.j);
+          else
+            row_g2s<L, R>(sr, in, x.j);
+        }
         __syncthreads();
         constexpr int NP = R / 2 + 1;
         cpx za[NP], zb[NP];
