@@ -293,6 +293,28 @@ class Workload2D:
         return t, 2.5 * n * math.log2(n) * 8 * threads * reps
 
 
+def alternate_plan_sets(torch, plans, like, nout):
+    """For each plan: its own CUDA stream, host-async mode and `nout` pinned
+    host arrays shaped like `like` (the plan's outputs on the steps it runs)."""
+    sets = []
+    for plan in plans:
+        st = torch.cuda.Stream()
+        plan.set_stream(st.cuda_stream)
+        plan.set_host_async(True)
+        sets.append((plan, st, [torch.empty_like(like, pin_memory=True) for _ in range(nout)]))
+    return sets
+
+
+def next_plan_set(w):
+    """The plan and host outputs of the next end-to-end step of workload w
+    (alternating between two sets); a set first waits for its previous step."""
+    plan, _, outs = w.e2e_sets[w.e2e_k & 1]
+    if w.e2e_k >= 2:
+        plan.synchronize()
+    w.e2e_k += 1
+    return plan, outs
+
+
 class WorkloadBatch4096:
     """1024 independent complex DFTs of length 4096 (c128), forward then inverse."""
 
@@ -338,17 +360,20 @@ class WorkloadBatch4096:
         return 2
 
     def e2e_setup(self):
+        """Two plans on their own streams in host-async mode, used on
+        alternate steps (see Workload3D256.e2e_setup)."""
         t = self.torch
         self.hx = t.empty(self.xs[0].shape, dtype=t.complex128, pin_memory=True)
         self.hx.copy_(self.xs[0].cpu())
-        self.hy = t.empty_like(self.hx, pin_memory=True)
-        self.hz = t.empty_like(self.hx, pin_memory=True)
+        self.e2e_sets = alternate_plan_sets(t, [self.plan, self.eng.plan("dft", (self.n,))], self.hx, 2)
+        self.e2e_k = 0
         b = self.hx.numel() * 16
         return 2 * b, 2 * b
 
     def e2e_step(self):
-        self.plan.batch("dft", self.hx.data_ptr(), self.hy.data_ptr(), self.howmany)
-        self.plan.batch("invdft", self.hy.data_ptr(), self.hz.data_ptr(), self.howmany)
+        plan, (hy, hz) = next_plan_set(self)
+        plan.batch("dft", self.hx.data_ptr(), hy.data_ptr(), self.howmany)
+        plan.batch("invdft", hy.data_ptr(), hz.data_ptr(), self.howmany)
 
     def config(self):
         return {"workload": "1024 x complex DFT N=4096 c128, forward then inverse", "n": self.n,
@@ -565,17 +590,21 @@ class Workload3D256:
         return sum(self.eng.launch_count(op, self.plan.aux) for op in ("dft", "invdft"))
 
     def e2e_setup(self):
+        """Two plans (same precision) on their own streams in host-async mode,
+        with their own pinned host outputs, used on alternate steps: a step's
+        upload overlaps the previous step's download."""
         t = self.torch
         self.hx = t.empty(self.dims, dtype=t.complex64, pin_memory=True)
         self.hx.copy_(self.xs[0].cpu())
-        self.hy = t.empty_like(self.hx, pin_memory=True)
-        self.hz = t.empty_like(self.hx, pin_memory=True)
+        self.e2e_sets = alternate_plan_sets(t, [self.plan, self._mkplan()], self.hx, 2)
+        self.e2e_k = 0
         b = self.hx.numel() * 8
         return 2 * b, 2 * b
 
     def e2e_step(self):
-        self.plan("dft", self.hx.data_ptr(), self.hy.data_ptr(), check=False)
-        self.plan("invdft", self.hy.data_ptr(), self.hz.data_ptr(), check=False)
+        plan, (hy, hz) = next_plan_set(self)
+        plan("dft", self.hx.data_ptr(), hy.data_ptr(), check=False)
+        plan("invdft", hy.data_ptr(), hz.data_ptr(), check=False)
 
     def config(self):
         return {"workload": "3-D complex DFT 256x256x256 c64, forward then inverse", "dims": list(self.dims),
@@ -925,6 +954,31 @@ def run_engine(args):
                      "gbs": round(by / (tot / cnt / 1e3) / 1e9, 1)} for lab, cnt, tot, by in stats]
 
     # end to end through the C ABI with pinned host buffers
+    def copy_floor_ms(h2d_bytes, d2h_bytes, reps=5):
+        """Milliseconds to move one step's input bytes host->device and its
+        output bytes device->host at the same time (pinned host memory, one
+        stream per direction, no kernels): the transfer floor of an
+        end-to-end step."""
+        hi = torch.empty(max(int(h2d_bytes), 16), dtype=torch.uint8).pin_memory()
+        di = torch.empty(hi.numel(), dtype=torch.uint8, device=dev)
+        ho = torch.empty(max(int(d2h_bytes), 16), dtype=torch.uint8).pin_memory()
+        do = torch.empty(ho.numel(), dtype=torch.uint8, device=dev)
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+        def once():
+            with torch.cuda.stream(s_in):
+                di.copy_(hi, non_blocking=True)
+            with torch.cuda.stream(s_out):
+                ho.copy_(do, non_blocking=True)
+
+        once()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(reps):
+            once()
+        torch.cuda.synchronize()
+        return 1000 * (time.perf_counter() - t) / reps
+
     e2e = None
     if not args.no_e2e:
         h2d, d2h = W.e2e_setup()
@@ -950,6 +1004,9 @@ def run_engine(args):
         e2e = {"value": round(flops_step * k_e2e * world / el / 1e9, 3), "unit": "GFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": k_e2e,
                "ms_per_step": round(1000 * el / k_e2e, 3)}
+        floor = copy_floor_ms(h2d, d2h)
+        e2e["copy_floor_ms_per_step"] = round(floor, 3)
+        e2e["frac_of_copy_floor"] = round(floor / (1000 * el / k_e2e), 4)
 
     # CPU baseline (rank 0, one GPU only): the reference on the host cores
     cpu = None
