@@ -11,6 +11,8 @@ enum Combo : int {
   K_DCT2,       // DCT-2 / DST-2 with fused permutation, unpacking and post-rotation
   K_DCT3,       // DCT-3 / DST-3 with fused pre-rotation, packing and de-interleave
   K_T4,         // DCT-4 / DST-4 with fused pre- and post-rotation
+  K_R2CQ,       // real DFT of 4 rows j + Q*m, then the first radix-4 stage of the column DFT across them
+  K_C2RQ,       // last radix-4 stage of an inverse column DFT across 4 rows, then their inverse real DFT
   K_COUNT
 };
 

@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <new>
@@ -423,8 +424,12 @@ struct Planner {
   }
 
   static bool staged(int combo) {
-    return combo == mb::K_R2C || combo == mb::K_C2R || combo == mb::K_DCT2 || combo == mb::K_DCT3;
+    return combo == mb::K_R2C || combo == mb::K_C2R || combo == mb::K_DCT2 || combo == mb::K_DCT3 ||
+           combo == mb::K_R2CQ || combo == mb::K_C2RQ;
   }
+
+  // the split-column kinds work on exactly four rows per CTA
+  static bool four_rows(int combo) { return combo == mb::K_R2CQ || combo == mb::K_C2RQ; }
 
   // default kernel form when no tuned configuration exists (the pipelined
   // form is chosen per launch by the autotuner; MINFFT_B200_PIPE=1 makes it
@@ -591,6 +596,10 @@ struct Planner {
         R = rr;
       }
     }
+    if (four_rows(combo)) {
+      ap.cpb = 4;
+      if (!mb::axis_kernel(combo, lg, R)) R = (R == 16) ? 8 : 16;
+    }
     Launch ln;
     ln.key = key;
     ln.radix = R;
@@ -622,19 +631,21 @@ struct Planner {
     ln.out_buf = out_buf;
     ln.vec_in = vec_in;
     ln.vec_out = vec_out;
-    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R);
-    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C);
+    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R || combo == mb::K_C2RQ);
+    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C || combo == mb::K_R2CQ);
     ln.combo = combo;
     ln.L = L;
     ln.ap = ap;
     {
-      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4"};
+      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4", "r2c+col4", "col4+c2r"};
       const double R = sizeof(real), C = sizeof(cpx);
       double per = 0;
       switch (combo) {
         case mb::K_CPLX: per = 2.0 * L * C; break;
-        case mb::K_R2C: per = 2.0 * L * R + (L + 1) * C; break;
-        case mb::K_C2R: per = (L + 1) * C + 2.0 * L * R; break;
+        case mb::K_R2C:
+        case mb::K_R2CQ: per = 2.0 * L * R + (L + 1) * C; break;
+        case mb::K_C2R:
+        case mb::K_C2RQ: per = (L + 1) * C + 2.0 * L * R; break;
         default: per = 4.0 * L * R; break;
       }
       ln.bytes = per * double(nbatch);
@@ -710,13 +721,13 @@ struct Planner {
     ln.in_buf = in_buf;
     ln.out_buf = out_buf;
     ln.vec_out = (combo == mb::K_C2R);
-    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R);
-    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C);
+    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R || combo == mb::K_C2RQ);
+    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C || combo == mb::K_R2CQ);
     ln.combo = combo;
     ln.L = L;
     ln.ap = ap;
     {
-      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4"};
+      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4", "r2c+col4", "col4+c2r"};
       const double Rb = sizeof(real), C = sizeof(cpx);
       double per = 0;
       switch (combo) {
@@ -848,6 +859,101 @@ struct Planner {
       if (!bad) return b;
     }
     return BUF_T4;
+  }
+
+  // 2-D real DFT of H arrays of Nr rows of N reals with a split column DFT:
+  // Nr = 4Q, the column DFT of length Nr done as a radix-4 stage fused into
+  // the row pass (four rows j + Q*m per CTA) and length-Q DFTs of the four
+  // blocks, so the column passes work on short columns with wide tiles.  Taken
+  // when the rows fit four to a CTA and Nr is at least MINFFT_B200_SPLIT2D
+  // (default 1024; 0 turns it off).
+  bool split_2d(int64_t Nr, int64_t N) const {
+    static const int64_t min_rows = [] {
+      const char* e = getenv("MINFFT_B200_SPLIT2D");
+      if (!e) return int64_t(1024);
+      const long long v = atoll(e);
+      return v <= 0 ? std::numeric_limits<int64_t>::max() : int64_t(v);
+    }();
+    const int64_t L = N / 2;
+    if (Nr < min_rows || Nr % 4 != 0 || L < 16 || L > 2048) return false;
+    if (ilog2(Nr / 4) > kColCapLog2) return false;
+    return mb::axis_pass_smem(int(L), int(std::min<int64_t>(16, L)), 4, 0) <= (size_t)dev_max_smem;
+  }
+
+  // Forward: rows X -> block layout in `mid` (row j of block q at (q*Q + j)*K),
+  // then length-Q column DFTs mid -> Y (output p of block q at row q + 4p).
+  void plan_realdft_split(int64_t H, int64_t Nr, int64_t N, int in_buf, int mid, int out_buf) {
+    const int64_t K = N / 2 + 1, Q = Nr / 4, L = N / 2;
+    AxisParams ap = base_params();
+    ap.d0 = 4;
+    ap.d1 = Q;
+    ap.is0 = Q * N;
+    ap.is1 = N;
+    ap.is2 = Nr * N;
+    ap.in_n = 1;
+    ap.os0 = Q * K;
+    ap.os1 = K;
+    ap.os2 = Nr * K;
+    ap.out_k = 1;
+    ap.cpb = 4;
+    ap.tw = tab(TB_TW, L);
+    ap.t1 = tab(TB_RFT, N);
+    ap.t2 = tab(TB_TW, Nr);
+    add_axis_kernel(mb::K_R2CQ, int(L), H * Nr, ap, in_buf, mid, true, false);
+    AxisParams cp = base_params();
+    cp.d0 = K;
+    cp.d1 = 4;
+    cp.is0 = 1;
+    cp.is1 = Q * K;
+    cp.is2 = Nr * K;
+    cp.in_n = K;
+    cp.os0 = 1;
+    cp.os1 = K;
+    cp.os2 = Nr * K;
+    cp.out_k = 4 * K;
+    cp.colmode = 1;
+    cp.cpb = choose_cpb(int(Q), true);
+    cp.tw = tab(TB_TW, Q);
+    add_axis_kernel(mb::K_CPLX, int(Q), H * 4 * K, cp, mid, out_buf, false, false);
+  }
+
+  // Inverse: length-Q inverse column DFTs of rows q + 4p, X -> block layout in
+  // `mid`, then the fused radix-4 stage and the inverse real DFTs of the rows,
+  // mid -> Y.
+  void plan_invrealdft_split(int64_t H, int64_t Nr, int64_t N, int in_buf, int mid, int out_buf) {
+    const int64_t K = N / 2 + 1, Q = Nr / 4, L = N / 2;
+    AxisParams cp = base_params();
+    cp.d0 = K;
+    cp.d1 = 4;
+    cp.is0 = 1;
+    cp.is1 = K;
+    cp.is2 = Nr * K;
+    cp.in_n = 4 * K;
+    cp.os0 = 1;
+    cp.os1 = Q * K;
+    cp.os2 = Nr * K;
+    cp.out_k = K;
+    cp.colmode = 1;
+    cp.flags = mb::F_CONJ_IN | mb::F_CONJ_OUT;
+    cp.cpb = choose_cpb(int(Q), true);
+    cp.tw = tab(TB_TW, Q);
+    add_axis_kernel(mb::K_CPLX, int(Q), H * 4 * K, cp, in_buf, mid, false, false);
+    AxisParams ap = base_params();
+    ap.d0 = 4;
+    ap.d1 = Q;
+    ap.is0 = Q * K;
+    ap.is1 = K;
+    ap.is2 = Nr * K;
+    ap.in_n = 1;
+    ap.os0 = Q * N;
+    ap.os1 = N;
+    ap.os2 = Nr * N;
+    ap.out_k = 1;
+    ap.cpb = 4;
+    ap.tw = tab(TB_TW, L);
+    ap.t1 = tab(TB_TW, Nr);
+    ap.t2 = tab(TB_RFT, N);
+    add_axis_kernel(mb::K_C2RQ, int(L), H * Nr, ap, mid, out_buf, false, true);
   }
 
   void plan_axis(const AxisStep& s) {
@@ -1085,6 +1191,11 @@ bool build_program(minfft_aux* a, int op, int howmany, bool alias, Program* prog
       std::vector<int64_t> H(D);
       H[nd - 1] = K;
       const size_t spec_bytes = size_t(prod(H, 0, nd)) * sizeof(cpx);
+      if (nd == 3 && pl.split_2d(D[1], N)) {
+        pl.need(BUF_T1, spec_bytes);
+        pl.plan_realdft_split(D[0], D[1], N, BUF_X, BUF_T1, BUF_Y);
+        break;
+      }
       AxisStep s{};
       s.combo = mb::K_R2C;
       s.N = N;
@@ -1105,6 +1216,11 @@ bool build_program(minfft_aux* a, int op, int howmany, bool alias, Program* prog
       std::vector<int64_t> H(D);
       H[nd - 1] = K;
       const size_t spec_bytes = size_t(prod(H, 0, nd)) * sizeof(cpx);
+      if (nd == 3 && pl.split_2d(D[1], N)) {
+        pl.need(BUF_T1, spec_bytes);
+        pl.plan_invrealdft_split(D[0], D[1], N, BUF_X, BUF_T1, BUF_Y);
+        break;
+      }
       int src = BUF_X;
       if (nd > 2) {
         pl.need(BUF_T1, spec_bytes);
@@ -1696,10 +1812,12 @@ Extent launch_extent(const Launch& ln) {
         e.out_max = oo + (L - 1) * ap.out_k;
         break;
       case mb::K_R2C:
+      case mb::K_R2CQ:  // d0 = 4: the largest batch offset is block 3's row
         e.in_max = oi + 2 * L - 1;
         e.out_max = oo + L * ap.out_k;
         break;
       case mb::K_C2R:
+      case mb::K_C2RQ:
         e.in_max = oi + L * ap.in_n;
         e.out_max = oo + 2 * L - 1;
         break;
@@ -1812,6 +1930,9 @@ MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns,
               size_t(ap.cpb) * mb::tile_pitch(ln.L, std::min(ln.radix, ln.L), ap.cpb, ap.colmode) * sizeof(cpx))
         fail("launch %zu: stage of %d bytes too small", i, ap.stage_bytes);
     }
+    if (!ln.is_line && (ln.combo == mb::K_R2CQ || ln.combo == mb::K_C2RQ) &&
+        (ln.ap.cpb != 4 || ln.ap.d0 != 4 || ln.ap.nbatch % 4 != 0 || ln.ap.colmode || ln.pipe))
+      fail("launch %zu (%s): split-column pass needs four rows j + Q*m per CTA", i, ln.label.c_str());
     if (ln.tc) {
       if (ln.L != mb::kTcLength || ln.combo != mb::K_CPLX || ln.ap.st_ns != 1)
         fail("launch %zu (%s): tensor-core pass on an unsupported axis", i, ln.label.c_str());
@@ -1898,6 +2019,7 @@ MB_EXPORT int minfft_b200_autotune(minfft_aux* a, int op, int howmany, int reps)
       const int pipe = cand & 1, radix = (cand & 2) ? 8 : 16;
       if (radix == 8 && key.L <= 8) continue;
       for (int cpb = 1; cpb <= probe.max_threads_cpb(key.L, radix); cpb *= 2) {
+        if (Planner::four_rows(key.combo) && (pipe || cpb != 4)) continue;
         const bool fits = pipe ? probe.pipe_fits(key.combo, key.L, cpb, key.colmode, radix)
                                : probe.plain_fits(key.combo, key.L, cpb, key.staged ? mb::F_STAGE_ROWS : 0,
                                                   key.colmode, radix);

@@ -234,6 +234,67 @@ def test_round_trips_scale_as_documented():
     assert rel_l2(y / (4 * n), xr) < 1e-14
 
 
+SPLIT_2D = [(1024, 32), (1024, 64), (2048, 256), (4096, 32), (1024, 4096)]
+
+
+def launch_labels(eng, plan, op, x_dev, y_dev):
+    eng.profile(plan.aux, 1)
+    plan(op, x_dev.data_ptr(), y_dev.data_ptr())
+    torch.cuda.synchronize()
+    labels = [st[0] for st in eng.profile_stats(plan.aux)]
+    eng.profile(plan.aux, 0)
+    return labels
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+@pytest.mark.parametrize("dims", SPLIT_2D, ids=lambda d: "x".join(map(str, d)))
+def test_split_column_real_dft_2d(dims, single):
+    """2-D real DFTs of at least 1024 rows split their column DFT: a radix-4
+    stage across rows j + Q*m fused into the row pass, length-rows/4 column
+    passes.  The launch list shows both fused kernels, and forward, inverse,
+    in-place, host-pointer and batched calls match the oracle, also after
+    autotuning (which keeps four rows per CTA)."""
+    rng = np.random.default_rng(sum(dims))
+    tol = tolerance(single, dims)
+    eng = minfft_b200.engine(single)
+    x = make_input("realdft", dims, rng, single)
+    z = make_input("invrealdft", dims, rng, single)
+    plan = eng.plan("realdft", dims)
+    try:
+        xt = torch.from_numpy(x).cuda()
+        zt = torch.from_numpy(z).cuda()
+        yt = torch.empty(z.shape, dtype=zt.dtype, device="cuda")
+        wt = torch.empty(x.shape, dtype=xt.dtype, device="cuda")
+        assert any(lab.startswith("axis_pass<r2c+col4") for lab in launch_labels(eng, plan, "realdft", xt, yt))
+        assert any(lab.startswith("axis_pass<col4+c2r") for lab in launch_labels(eng, plan, "invrealdft", zt, wt))
+        for _ in range(2):  # as planned, then with the autotuner's configurations
+            plan("realdft", xt.data_ptr(), yt.data_ptr())
+            plan("invrealdft", zt.data_ptr(), wt.data_ptr())
+            torch.cuda.synchronize()
+            assert rel_l2(yt.cpu().numpy(), expected("realdft", x, dims)) <= tol
+            assert rel_l2(wt.cpu().numpy(), expected("invrealdft", z, dims)) <= tol
+            assert torch.equal(zt.cpu(), torch.from_numpy(z)), "inverse input was modified"
+            eng.autotune(plan.aux, "realdft", 1, 2)
+            eng.autotune(plan.aux, "invrealdft", 1, 2)
+        # a batch of three arrays through one call
+        xb = np.stack([make_input("realdft", dims, rng, single) for _ in range(3)])
+        xbt = torch.from_numpy(xb).cuda()
+        ybt = torch.empty((3,) + z.shape, dtype=zt.dtype, device="cuda")
+        plan.batch("realdft", xbt.data_ptr(), ybt.data_ptr(), 3)
+        torch.cuda.synchronize()
+        yb = ybt.cpu().numpy()
+        for i in range(3):
+            assert rel_l2(yb[i], expected("realdft", xb[i], dims)) <= tol, i
+    finally:
+        plan.free()
+    for op, inp in (("realdft", x), ("invrealdft", z)):
+        ref = expected(op, inp, dims)
+        assert rel_l2(gpu_apply(op, inp, dims, single, inplace=True), ref) <= tol, (op, "in place")
+        assert rel_l2(gpu_apply(op, inp, dims, single, host=True), ref) <= tol, (op, "host")
+    y = gpu_apply("invrealdft", gpu_apply("realdft", x.astype(np.float64), dims, False), dims, False)
+    assert rel_l2(y / np.prod(dims), x) < 1e-14
+
+
 # --------------------------------------------------------- workload sizes
 @pytest.mark.slow
 @pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
