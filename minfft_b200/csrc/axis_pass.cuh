@@ -580,38 +580,42 @@ struct LoadC2R {
 // element stride in_n) receive the last radix-4 stage of the inverse column
 // DFTs from row j of the four blocks V_q left by the length-Q inverse DFTs,
 //   X_m = sum_q w_4^(-m*q) (w_Nr^(-j*q) V_q),
-// staged in the tile (X_L in the row's spare slot 16), then packed for their
-// inverse real DFTs as LoadC2R does.  t1 = w_Nr^n, t2 = w_N^k.
+// and are packed for their inverse real DFTs as LoadC2R does.  One pass over
+// the spectrum pairs (k, L-k) covers all four rows: each thread forms both
+// columns of the pair for every row and packs them (one root w_N^k for all
+// four).  t1 = w_Nr^n, t2 = w_N^k.
 struct LoadC2RQ {
   static constexpr bool kStaged = true;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
-    static_assert(L >= 16, "the spare slot 16 of a tile row holds X_L");
     constexpr int NT = 4 * (L / R);  // threads of the CTA (four transforms)
     const cpx* in = static_cast<const cpx*>(p.in) + (x.oin - int64_t(x.c) * p.is0);  // row j of block 0
     const int64_t jr = (x.b / p.d0) % p.d1;  // the CTA's row index j
     const cpx w1 = cconj(ldg(p.t1 + jr)), w2 = cconj(ldg(p.t1 + 2 * jr)), w3 = cconj(ldg(p.t1 + 3 * jr));
     const int64_t bs = p.is0;
+    // column col of the four blocks -> the four rows' spectra at col
+    auto gather4 = [&](int col, cpx (&X)[4]) {
+      const cpx* q = in + int64_t(col) * p.in_n;
+      const cpx u0 = q[0], u1 = cmul(q[bs], w1), u2 = cmul(q[2 * bs], w2), u3 = cmul(q[3 * bs], w3);
+      const cpx a0 = cadd(u0, u2), a1 = csub(u0, u2), c0 = cadd(u1, u3), c1 = csub(u1, u3);
+      const cpx ic1 = cmk(-c1.y, c1.x);  // i * c1
+      X[0] = cadd(a0, c0);
+      X[1] = cadd(a1, ic1);
+      X[2] = csub(a0, c0);
+      X[3] = csub(a1, ic1);
+    };
 #pragma unroll
-    for (int it = 0; it < (L + NT) / NT; ++it) {
-      const int k = threadIdx.x + it * NT;
-      if (k <= L) {
-        const cpx* q = in + int64_t(k) * p.in_n;
-        const cpx u0 = q[0], u1 = cmul(q[bs], w1), u2 = cmul(q[2 * bs], w2), u3 = cmul(q[3 * bs], w3);
-        const cpx a0 = cadd(u0, u2), a1 = csub(u0, u2), c0 = cadd(u1, u3), c1 = csub(u1, u3);
-        const cpx ic1 = cmk(-c1.y, c1.x);  // i * c1
-        const int sl = k < L ? pad16(k) : 16;
-        t.s[sl] = cadd(a0, c0);
-        t.s[t.lp + sl] = cadd(a1, ic1);
-        t.s[2 * t.lp + sl] = csub(a0, c0);
-        t.s[3 * t.lp + sl] = csub(a1, ic1);
+    for (int it = 0; it < (L / 2 + NT) / NT; ++it) {
+      const int k = threadIdx.x + it * NT;  // pair (k, L-k), k = 0 .. L/2
+      if (k <= L / 2) {
+        cpx Xa[4], Xb[4];
+        gather4(k, Xa);
+        if (2 * k != L) gather4(k == 0 ? L : L - k, Xb);  // X_L pairs with X_0
+        const cpx f = (k > 0 && 2 * k < L) ? ldg(p.t2 + k) : cmk(real(1), real(0));
+#pragma unroll
+        for (int m = 0; m < 4; ++m) pack_into(t, m, k, L, Xa[m], Xb[m], f);
       }
     }
-    __syncthreads();
-    const cpx b2 = kind_base<L / R>(p.t2, x.j);
-    const cpx* row = t.s + x.c * t.lp;
-    pair_loop<L, R>(x, [&](int k) { return row[k == L ? 16 : pad16(k)]; },
-                    [&](int i, int k, cpx z0, cpx z1) { pack_into(t, x.c, k, L, z0, z1, rft_root<R>(b2, i)); });
     __syncthreads();
     gather_natural<L, R>(v, x.j, x.c, t);
   }
@@ -827,56 +831,63 @@ struct StoreDCT2 {
 // forward result) read as interleaved reals (reference minfft.c:605,658).
 // Split column DFT of a 2-D real DFT with Nr = 4Q rows, forward half.  The
 // CTA holds the four rows j + Q*m (transform c = m: batch layout d0 = 4 with
-// is0 = Q rows, d1 = Q with is1 = one row, cpb = 4).  After their real DFTs it
-// applies the first radix-4 stage of the length-Nr column DFTs across them,
-//   Z_q[j] = w_Nr^(j*q) * sum_m X_m w_4^(m*q)      (X_m = spectrum of row j + Q*m),
+// is0 = Q rows, d1 = Q with is1 = one row, cpb = 4).  After their half-length
+// DFTs it applies, column by column, the first radix-4 stage of the length-Nr
+// column DFTs across the four rows' spectra X_m,
+//   Z_q[j] = w_Nr^(j*q) * sum_m X_m w_4^(m*q),
 // and writes Z_q to row j of block q of the output (block stride os0, element
 // stride out_k); length-Q DFTs of each block then finish the column DFTs
-// (their output p is row q + 4p).  t1 = w_N^k (real-DFT table), t2 = w_Nr^n.
-// The spectrum is unpacked into the tile in place, X_L into the row's spare
-// slot 16 (pad16 never addresses it).
+// (their output p is row q + 4p).  One pass over the spectrum pairs (k, L-k)
+// covers all four rows: each thread unpacks the pair for every row (one root
+// w_N^k for all four) and stores both columns.  t1 = w_N^k (real-DFT table),
+// t2 = w_Nr^n.
 struct StoreR2CQ {
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, const TileOffsets& to,
                                              cpx (&v)[R]) {
-    static_assert(L >= 16, "the spare slot 16 of a tile row holds X_L");
     constexpr int NT = 4 * (L / R);  // threads of the CTA (four transforms)
     __syncthreads();
     scatter_natural<L, R>(v, x.j, x.c, t);
-    __syncthreads();
-    const cpx b1 = kind_base<L / R>(p.t1, x.j);
-    cpx* row = t.s + x.c * t.lp;
-    pair_loop<L, R>(x, [&](int k) { return t.s[t.idx(x.c, k & (L - 1))]; }, [&](int i, int k, cpx za, cpx zb) {
-      if (k == 0) {
-        row[0] = cmk(za.x + za.y, real(0));
-        row[16] = cmk(za.x - za.y, real(0));
-      } else if (2 * k == L) {
-        row[pad16(k)] = cconj(za);
-      } else {
-        cpx xa, xb;
-        unpack_pair(za, zb, rft_root<R>(b1, i), xa, xb);
-        row[pad16(k)] = xa;
-        row[pad16(L - k)] = xb;
-      }
-    });
     __syncthreads();
     const int64_t jr = (x.b / p.d0) % p.d1;  // the CTA's row index j
     const cpx w1 = ldg(p.t2 + jr), w2 = ldg(p.t2 + 2 * jr), w3 = ldg(p.t2 + 3 * jr);
     cpx* out = static_cast<cpx*>(p.out) + to.out_off[0];  // row j of block 0
     const int64_t bs = p.os0;
+    // column col of the four rows -> blocks 0..3
+    auto emit = [&](int col, const cpx (&X)[4]) {
+      const cpx a0 = cadd(X[0], X[2]), a1 = csub(X[0], X[2]), c0 = cadd(X[1], X[3]), c1 = csub(X[1], X[3]);
+      const cpx mic1 = cmk(c1.y, -c1.x);  // -i * c1
+      cpx* q = out + int64_t(col) * p.out_k;
+      q[0] = cadd(a0, c0);
+      q[bs] = cmul(cadd(a1, mic1), w1);
+      q[2 * bs] = cmul(csub(a0, c0), w2);
+      q[3 * bs] = cmul(csub(a1, mic1), w3);
+    };
 #pragma unroll
-    for (int it = 0; it < (L + NT) / NT; ++it) {
-      const int k = threadIdx.x + it * NT;
-      if (k <= L) {
-        const int sl = k < L ? pad16(k) : 16;
-        const cpx s0 = t.s[sl], s1 = t.s[t.lp + sl], s2 = t.s[2 * t.lp + sl], s3 = t.s[3 * t.lp + sl];
-        const cpx a0 = cadd(s0, s2), a1 = csub(s0, s2), c0 = cadd(s1, s3), c1 = csub(s1, s3);
-        const cpx mic1 = cmk(c1.y, -c1.x);  // -i * c1
-        cpx* q = out + int64_t(k) * p.out_k;
-        q[0] = cadd(a0, c0);
-        q[bs] = cmul(cadd(a1, mic1), w1);
-        q[2 * bs] = cmul(csub(a0, c0), w2);
-        q[3 * bs] = cmul(csub(a1, mic1), w3);
+    for (int it = 0; it < (L / 2 + NT) / NT; ++it) {
+      const int k = threadIdx.x + it * NT;  // pair (k, L-k), k = 0 .. L/2
+      if (k <= L / 2) {
+        cpx Xa[4], Xb[4];
+        if (k == 0) {
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            const cpx z = t.s[t.idx(m, 0)];
+            Xa[m] = cmk(z.x + z.y, real(0));
+            Xb[m] = cmk(z.x - z.y, real(0));  // X_L
+          }
+          emit(0, Xa);
+          emit(L, Xb);
+        } else if (2 * k == L) {
+#pragma unroll
+          for (int m = 0; m < 4; ++m) Xa[m] = cconj(t.s[t.idx(m, k)]);
+          emit(k, Xa);
+        } else {
+          const cpx f = ldg(p.t1 + k);
+#pragma unroll
+          for (int m = 0; m < 4; ++m) unpack_pair(t.s[t.idx(m, k)], t.s[t.idx(m, L - k)], f, Xa[m], Xb[m]);
+          emit(k, Xa);
+          emit(L - k, Xb);
+        }
       }
     }
   }
