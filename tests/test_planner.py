@@ -56,6 +56,36 @@ def test_2d_workload_launch_counts():
             assert bad == 0 and n == 2, (op, n, rep)
 
 
+SPLIT_2D = [(1024, 32), (1024, 64), (2048, 2048), (4096, 32), (1024, 4096), (16384, 32)]
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["double", "single"])
+def test_split_column_real_dft_plans(single):
+    """2-D real DFTs of >= 1024 rows split the column DFT into a radix-4 stage
+    fused into the row pass and length-rows/4 column passes: two launches per
+    direction, in bounds for single and batched calls, in place or not, and
+    whatever tile size or radix the autotuner forces (the fused row passes
+    keep four rows per CTA)."""
+    eng = minfft_b200.engine(single)
+    try:
+        for forced in ((-1, 0, 16), (0, 1, 16), (0, 8, 8), (0, 32, 16), (1, 4, 16)):
+            eng.tune_set_default(*forced)
+            for dims in SPLIT_2D:
+                for op in ("realdft", "invrealdft"):
+                    for howmany in (1, 3):
+                        for alias in (False, True):
+                            bad, rep, n = eng.plan_selfcheck(op, dims, howmany, alias)
+                            assert bad == 0, (forced, op, dims, howmany, alias, rep)
+                            assert n == 2, (forced, op, dims, howmany, n)
+        # below the row threshold, or rows too short for four per CTA: the plain plan
+        eng.tune_set_default(-1, 0)
+        for dims in ((512, 64), (2048, 16)):
+            bad, rep, n = eng.plan_selfcheck("realdft", dims, 1, False)
+            assert bad == 0 and n == 2, (dims, n, rep)
+    finally:
+        eng.tune_set_default(-1, 0)
+
+
 def test_selfcheck_rejects_bad_arguments():
     eng = minfft_b200.engine(False)
     assert eng.plan_selfcheck("dft", (12,))[0] == -1
