@@ -11,7 +11,13 @@ engine's C ABI on device-resident data.  Metric: GFLOP/s with the
 2.5 * N * log2(N) convention for real-data transforms (N = 2^22 points).
 
 Other workloads (``--workload``): "batch4096" (1024 complex DFTs of length
-4096, c128, forward then inverse; 5 N log2 N per transform).
+4096, c128, forward then inverse; 5 N log2 N per transform), "mixed20000"
+(20000 1-D transforms of mixed kinds and lengths in one persistent launch),
+"3d256" (256^3 c64 DFT, forward then inverse), "long1d" (2^26-point DFTs in
+c128 and c64, 2^24-point DCT-4/DST-4 in f64 and f32) and "long1d_c64" (the
+2^26-point c64 DFT, forward then inverse).  "3d256" and "long1d_c64" take
+``--precision fp32|tc_f16|tc_bf16`` (CUDA-core or tensor-core split-precision
+256-point passes).
 
 Timing: W untimed warm-up steps, then exactly K steps between CUDA events on
 the stream the kernels run on (the legacy default stream), bracketed by a
@@ -783,8 +789,41 @@ class WorkloadLong1D(PerPrecisionStreams):
         return t, (2 * fd + 4 * f4) * P * reps
 
 
+class WorkloadLong1DC64(Workload3D256):
+    """Complex DFT of 2^26 points in c64, forward then inverse: a Stockham
+    chain of three passes over HBM.  --precision "tc_f16" / "tc_bf16" splits
+    the chain into two 256-point tensor-core passes (the second pre-twiddled)
+    and one 1024-point CUDA-core pass; "fp32" runs 512-, 512- and 256-point
+    CUDA-core passes."""
+
+    name = "long1d_c64"
+    dims = (1 << 26,)
+    nsets = 3
+
+    def config(self):
+        return {"workload": "1-D complex DFT N=2^26 c64, forward then inverse", "dims": list(self.dims),
+                "precision": self.precision,
+                "rel_l2_vs_f64_engine": self.err, "roundtrip_rel_l2": self.roundtrip,
+                "flops": "5*N*log2(N) per transform, N=2^26",
+                "inputs": "re/im i.i.d. standard normal, numpy PCG64 seed 3",
+                "l2": "inputs rotate over 3 sets of 512 MiB, larger than the 126 MB L2"}
+
+    @classmethod
+    def cpu_sample(cls, P):
+        return f"{min(P, 4)} concurrent instances (one per OpenMP thread, own plans) of dft + invdft, per timed step"
+
+    @classmethod
+    def cpu_measure(cls, kind, threads, warm, reps):
+        """A bounded sample: min(threads, 4) concurrent instances (a 2^26
+        transform holds 2 GiB of host memory in the single build)."""
+        P = min(threads, 4)
+        t = cpu_run(kind, cls.cpu_sequences, cls.dims, P, P, reps, warm)
+        n = int(np.prod(cls.dims))
+        return t, 5.0 * n * math.log2(n) * 2 * P * reps
+
+
 WORKLOADS = {"2d2048": Workload2D, "batch4096": WorkloadBatch4096, "mixed20000": WorkloadMixed,
-             "3d256": Workload3D256, "long1d": WorkloadLong1D}
+             "3d256": Workload3D256, "long1d": WorkloadLong1D, "long1d_c64": WorkloadLong1DC64}
 
 
 # -------------------------------------------------------------- CPU timing
@@ -866,6 +905,9 @@ def _ref_config(W):
     if W.name == "3d256":
         return {"workload": "3-D complex DFT 256x256x256 c64, forward then inverse", "dims": list(W.dims),
                 "precision": "f32 (reference single-precision build)", "flops": "5*N*log2(N) per transform, N=2^24"}
+    if W.name == "long1d_c64":
+        return {"workload": "1-D complex DFT N=2^26 c64, forward then inverse", "dims": list(W.dims),
+                "precision": "f32 (reference single-precision build)", "flops": "5*N*log2(N) per transform, N=2^26"}
     if W.name == "long1d":
         return {"workload": "1-D dft 2^26 (c128, c64) + dct4/dst4 2^24 (f64, f32)", "n_dft": W.n_dft,
                 "n_t4": W.n_t4, "transforms_per_step": 6, "flops": "5*N*log2(N) dft, 2.5*N*log2(N) dct4/dst4"}
@@ -1096,7 +1138,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (heuristic launch configurations)")
     ap.add_argument("--tune-file", default="", help="tuning table prefix: loaded if present, else saved after tuning")
     ap.add_argument("--precision", choices=["fp32", "tc_f16", "tc_bf16"], default="fp32",
-                    help="3d256: arithmetic of the 256-point axis passes")
+                    help="3d256, long1d_c64: arithmetic of the 256-point axis passes")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -468,12 +468,32 @@ struct Planner {
            sm <= (size_t)dev_max_smem;
   }
 
-  // The tensor-core pass covers complex 256-point axes without a
-  // pre-twiddle (every in-CTA axis of that length and the first pass of a
-  // Stockham chain); it always stages the tile through shared memory.
+  // The tensor-core pass covers complex 256-point axes: every in-CTA axis
+  // of that length and every 256-point pass of a Stockham chain over HBM
+  // (pre-twiddled in FP32 after the first); it always stages the tile
+  // through shared memory.
   bool use_tc(int combo, int L, const AxisParams& ap) const {
-    return a->precision != MINFFT_B200_PREC_FP32 && combo == mb::K_CPLX && L == mb::kTcLength && ap.st_ns == 1 &&
+    return a->precision != MINFFT_B200_PREC_FP32 && combo == mb::K_CPLX && L == mb::kTcLength &&
            (ap.flags & ~(mb::F_CONJ_IN | mb::F_CONJ_OUT | mb::F_STAGE_ROWS)) == 0;
+  }
+
+  // Sub-DFT lengths (log2) of the P passes of a Stockham chain over
+  // 2^bits points: as even as possible, the longer ones first; in a
+  // tensor-core precision mode, as many 256-point passes (first) as the
+  // same number of passes allows, the rest split evenly after them.
+  std::vector<int> pass_bits(int bits, int P) const {
+    const int tb = ilog2(mb::kTcLength);
+    int k = 0;
+    if (a->precision != MINFFT_B200_PREC_FP32) {
+      for (k = std::min(P, bits / tb); k > 0; --k) {
+        const int rest = bits - tb * k, left = P - k;
+        if (left == 0 ? rest == 0 : (rest >= left && rest <= left * kPassCapLog2)) break;
+      }
+    }
+    std::vector<int> pb(k, tb);
+    const int left = P - k, rest = bits - tb * k;
+    for (int p = 0; p < left; ++p) pb.push_back(rest / left + (p < rest % left ? 1 : 0));
+    return pb;
   }
 
   void add_tc_kernel(int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, const TuneKey& key) {
@@ -1006,8 +1026,7 @@ struct Planner {
   void plan_multipass(const AxisStep& s, int64_t Lt) {
     const int bits = ilog2(Lt);
     const int P = (bits + kPassCapLog2 - 1) / kPassCapLog2;
-    std::vector<int> pb(P, bits / P);
-    for (int p = 0; p < bits % P; ++p) pb[p] += 1;
+    const std::vector<int> pb = pass_bits(bits, P);
     const int64_t inner = s.inner, outer = s.outer;
     const int64_t Lp = Lt * inner;
     const size_t work_bytes = size_t(outer) * size_t(Lp) * sizeof(cpx);
@@ -1934,7 +1953,7 @@ MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns,
         (ln.ap.cpb != 4 || ln.ap.d0 != 4 || ln.ap.nbatch % 4 != 0 || ln.ap.colmode || ln.pipe))
       fail("launch %zu (%s): split-column pass needs four rows j + Q*m per CTA", i, ln.label.c_str());
     if (ln.tc) {
-      if (ln.L != mb::kTcLength || ln.combo != mb::K_CPLX || ln.ap.st_ns != 1)
+      if (ln.L != mb::kTcLength || ln.combo != mb::K_CPLX)
         fail("launch %zu (%s): tensor-core pass on an unsupported axis", i, ln.label.c_str());
       if (ln.ap.cpb != 8 && ln.ap.cpb != 16) fail("launch %zu: tensor-core tile of %d transforms", i, ln.ap.cpb);
       if (ln.ap.ntiles * ln.ap.cpb < ln.ap.nbatch || ln.grid < 1 || int64_t(ln.grid) > ln.ap.ntiles)

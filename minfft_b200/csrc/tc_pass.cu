@@ -32,6 +32,11 @@
 // two K steps of A0 B0 to round at full magnitude.  The unscaling and the
 // twiddles between the stages also run on the CUDA cores.
 //
+// In a later pass of a Stockham FFT over HBM (st_ns > 1) every input element
+// is first multiplied in FP32 by its pre-twiddle w_Lt^(n * gq), read as the
+// product of a coarse and a fine table root, before the scale is chosen; the
+// CUDA-core pass applies the same factors.
+//
 // Synchronisation: warp 0 allocates and frees the TMEM columns; thread 0
 // issues the MMAs and commits them to an mbarrier; every thread waits on it
 // with a bounded spin.  A wait that runs out records the failure in
@@ -109,7 +114,8 @@ struct TcLayout {
   static constexpr int region = a_bytes > d_bytes ? a_bytes : d_bytes;
   static constexpr int b_off = region;
   static constexpr int offs_off = b_off + NT * kBBytes;
-  static constexpr int mbar_off = offs_off + 4 * TB * 8;  // two sets of tile offsets
+  static constexpr int gq_off = offs_off + 4 * TB * 8;  // two sets of tile offsets
+  static constexpr int mbar_off = gq_off + 2 * TB * 8;   // two sets of pre-twiddle steps
   static constexpr int inv_off = mbar_off + 16;  // per-transform unscale factors
   static constexpr int total = inv_off + (TB * 4 + 15) / 16 * 16;
   static constexpr int tmem_cols = 64 * G;  // per group: leading accumulator, correction accumulator
@@ -211,16 +217,26 @@ __device__ __forceinline__ void load_tile(const AxisParams& p, const int64_t* of
   }
 }
 
-// Offsets of the TB transforms of tile `tile` (threads 0..TB-1).
+// Offsets of the TB transforms of tile `tile` (threads 0..TB-1), and, in a
+// later pass of a Stockham FFT over HBM, each transform's pre-twiddle step
+// gq = q << st_shift (its element n is multiplied by w_Lt^(n * gq), q the
+// span index).
 template <int TB>
-__device__ __forceinline__ void tile_offsets(const AxisParams& p, int64_t tile, int tid, int64_t* offs) {
+__device__ __forceinline__ void tile_offsets(const AxisParams& p, int64_t tile, int tid, int64_t* offs, int64_t* gq) {
   if (tid < TB) {
     const int64_t b = tile * TB + tid;
     int64_t b0, oi, oo;
     batch_offsets(p, b < p.nbatch ? b : 0, b0, oi, oo);
     offs[tid] = oi;
     offs[TB + tid] = oo;
+    gq[tid] = p.st_ns > 1 ? ((b0 / p.st_div) & (p.st_ns - 1)) << p.st_shift : 0;
   }
+}
+
+// w_Lt^g as the product of a coarse and a fine table root
+__device__ __forceinline__ cpx stockham_root(const AxisParams& p, int64_t g) {
+  const int64_t lomask = (int64_t(1) << p.st_lobits) - 1;
+  return cmul(ldg(p.st_hi + (g >> p.st_lobits)), ldg(p.st_lo + (g & lomask)));
 }
 
 // Persistent: CTA k handles tiles k, k + gridDim.x, ...; while the tensor
@@ -235,6 +251,7 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
   cpx* data = reinterpret_cast<cpx*>(sm);
   unsigned char* bop = sm + Lay::b_off;
   int64_t* offs = reinterpret_cast<int64_t*>(sm + Lay::offs_off);  // two sets of 2*TB (tile parity)
+  int64_t* gqs = reinterpret_cast<int64_t*>(sm + Lay::gq_off);     // two sets of TB (tile parity)
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + Lay::mbar_off);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + Lay::mbar_off + 8);
   int* bad = reinterpret_cast<int*>(sm + Lay::mbar_off + 12);
@@ -264,13 +281,14 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
     for (int i = tid; i < NT * kBBytes / 16; i += NTHR) dst[i] = src[i];
   }
   int64_t tile = blockIdx.x;
-  tile_offsets<TB>(p, tile, tid, offs);
+  tile_offsets<TB>(p, tile, tid, offs, gqs);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
 
   const bool cj_in = (p.flags & F_CONJ_IN) != 0, cj_out = (p.flags & F_CONJ_OUT) != 0;
+  const bool twid = p.st_ns > 1;
   constexpr uint32_t idesc = instr_desc<FMT>();
   const uint32_t aop_a = static_cast<uint32_t>(__cvta_generic_to_shared(aop));
   const uint32_t bop_a = static_cast<uint32_t>(__cvta_generic_to_shared(bop));
@@ -289,8 +307,9 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
 #pragma unroll 1
   for (int par = 0; tile < ntiles && ok; tile += gridDim.x, par ^= 1) {
     const int64_t* cur = offs + par * 2 * TB;
+    const int64_t* cur_gq = gqs + par * TB;
     // ---- the tile's inputs into shared memory (the previous tile's store
-    // has finished reading it)
+    // has finished reading it), pre-twiddled in FP32 in a later HBM pass
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int e = tid + i * NTHR;
@@ -298,11 +317,12 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
       const int n = p.colmode ? (e / TB) : (e % kL);
       cpx x = v[i];
       if (cj_in) x.y = -x.y;
+      if (twid) x = cmul(x, stockham_root(p, int64_t(n) * cur_gq[c]));
       data[c * kLP + pad16(n)] = x;
     }
     const int64_t next = tile + gridDim.x;
     int64_t* nxt = offs + (par ^ 1) * 2 * TB;
-    if (next < ntiles) tile_offsets<TB>(p, next, tid, nxt);
+    if (next < ntiles) tile_offsets<TB>(p, next, tid, nxt, gqs + (par ^ 1) * TB);
     __syncthreads();
     // ---- the next tile's loads are issued now and land during the stages
     if (next < ntiles) load_tile<TB>(p, nxt, valid(next), tid, v);

@@ -3,8 +3,8 @@ double-precision oracle, through the C ABI of the single-precision library.
 
 Every complex 256-point axis runs on tcgen05 in the TC modes: rows and
 columns of 1-D to 3-D arrays, ragged batches (ending inside a CTA tile),
-in-place calls, inverse transforms, and the first pass of a Stockham
-chain over HBM.  Bar: relative L2 error against the FP64 oracle at most 1e-6
+in-place calls, inverse transforms, and the 256-point passes of Stockham
+chains over HBM (the first, and the pre-twiddled later ones).  Bar: relative L2 error against the FP64 oracle at most 1e-6
 (tighter than the FP32 bar of 1e-6 * log2 N), and no wait of the kernel ran
 out (minfft_b200_tc_status)."""
 import numpy as np
@@ -106,8 +106,8 @@ def test_tc_uses_tensor_core_kernels(mode):
 
 
 @pytest.mark.parametrize("mode", MODES)
-def test_tc_first_pass_of_long_column_axis(mode):
-    """65536-point columns: two HBM passes of 256, the first on tensor cores."""
+def test_tc_passes_of_long_column_axis(mode):
+    """65536-point columns: two HBM passes of 256, both on tensor cores."""
     dims = (65536, 2)
     names = labels(dims, mode)
     assert any(n.startswith("tc_pass<") for n in names), names
@@ -115,6 +115,40 @@ def test_tc_first_pass_of_long_column_axis(mode):
     got = run("dft", x, dims, mode)
     err = rel_l2(got, ref("dft", x, dims))
     assert err <= 2 * TC_BAR, err
+
+
+# (dims, tensor-core launches per call): 2^16 = 256 x 256 (both passes, the
+# second pre-twiddled), 2^20 = 256 x 4096, 2^25 = 256 x 256 x 512, and
+# 131072-point columns of four = 256 x 512
+LONG_CHAINS = [((1 << 16,), 2), ((1 << 20,), 1), ((1 << 25,), 2), ((1 << 17, 4), 1)]
+
+
+def tc_launches(dims, mode, op="dft"):
+    eng = minfft_b200.engine(True)
+    plan = eng.plan("dft", dims)
+    try:
+        eng.set_precision(plan.aux, mode)
+        x = torch.zeros(dims, dtype=torch.complex64, device="cuda")
+        y = torch.empty_like(x)
+        eng.profile(plan.aux, 1)
+        plan(op, x.data_ptr(), y.data_ptr())
+        return sum(s[1] for s in eng.profile_stats(plan.aux) if s[0].startswith("tc_pass<"))
+    finally:
+        plan.free()
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("dims,ntc", LONG_CHAINS, ids=["x".join(map(str, d)) for d, _ in LONG_CHAINS])
+def test_tc_passes_of_long_chains(dims, ntc, mode):
+    """Axes beyond one CTA run as Stockham chains over HBM; in a TC mode the
+    chain holds as many 256-point passes as its pass count allows, all on
+    tensor cores, the later ones pre-twiddled in FP32 before the split."""
+    assert tc_launches(dims, mode) == ntc
+    x = data(dims, 11)
+    for op in ("dft", "invdft"):
+        got = run(op, x, dims, mode)
+        err = rel_l2(got, ref(op, x, dims))
+        assert err <= 2 * TC_BAR, (op, err)
 
 
 def run_rows(op, x, mode):

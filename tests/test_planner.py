@@ -111,14 +111,16 @@ def test_every_launch_configuration_is_in_bounds(single, pipe, radix):
 
 
 TC_SHAPES = [(256,), (4, 256), (256, 2), (256, 256), (256, 256, 256), (64, 64, 256), (256, 16, 4), (65536, 2),
-             (1 << 16,), (1 << 24,), (2, 256, 2)]
+             (1 << 16,), (1 << 24,), (2, 256, 2), (1 << 13,), (1 << 20,), (1 << 25,), (1 << 26,), (1 << 17, 4)]
 
 
 @pytest.mark.parametrize("precision", ["tc_f16", "tc_bf16"])
 @pytest.mark.parametrize("dims", TC_SHAPES, ids=lambda d: "x".join(map(str, d)))
 def test_tensor_core_plans_are_in_bounds(dims, precision):
-    """The tensor-core passes replace every complex 256-point axis pass without
-    a pre-twiddle; the plans stay sound and keep their launch counts."""
+    """The tensor-core passes replace every complex 256-point axis pass, the
+    pre-twiddled passes of Stockham chains over HBM included (a chain in a
+    tensor-core mode is split into as many 256-point passes as its pass count
+    allows); the plans stay sound and keep their launch counts."""
     eng = minfft_b200.engine(True)
     for op in OPS:
         for howmany, alias in itertools.product((1, 3), (False, True)):
