@@ -310,15 +310,45 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
     const int64_t* cur_gq = gqs + par * TB;
     // ---- the tile's inputs into shared memory (the previous tile's store
     // has finished reading it), pre-twiddled in FP32 in a later HBM pass
+    if (twid && p.colmode) {
+      // column mode: this thread's 16 values are elements n0 + 16*i of
+      // transform tid % TB, so their roots are w^(n0*gq) * d^i with
+      // d = w^(16*gq): three table roots (w^(n0*gq), d, d^4), the other
+      // powers of d as at most two products
+      const int64_t gq = cur_gq[tid % TB];
+      const cpx base = stockham_root(p, int64_t(tid / TB) * gq);
+      const cpx d1 = stockham_root(p, 16 * gq);
+      const cpx d2 = cmul(d1, d1);
+      const cpx d3 = cmul(d2, d1);
+      const cpx d4 = stockham_root(p, 64 * gq);
+      const cpx d8 = cmul(d4, d4);
+      const cpx d12 = cmul(d8, d4);
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int e = tid + i * NTHR;
-      const int c = p.colmode ? (e % TB) : (e / kL);
-      const int n = p.colmode ? (e / TB) : (e % kL);
-      cpx x = v[i];
-      if (cj_in) x.y = -x.y;
-      if (twid) x = cmul(x, stockham_root(p, int64_t(n) * cur_gq[c]));
-      data[c * kLP + pad16(n)] = x;
+      for (int i = 0; i < 16; ++i) {
+        const int e = tid + i * NTHR;
+        const int c = e % TB, n = e / TB;
+        cpx w = base;
+        if ((i >> 2) == 1) w = cmul(w, d4);
+        if ((i >> 2) == 2) w = cmul(w, d8);
+        if ((i >> 2) == 3) w = cmul(w, d12);
+        if ((i & 3) == 1) w = cmul(w, d1);
+        if ((i & 3) == 2) w = cmul(w, d2);
+        if ((i & 3) == 3) w = cmul(w, d3);
+        cpx x = v[i];
+        if (cj_in) x.y = -x.y;
+        data[c * kLP + pad16(n)] = cmul(x, w);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int e = tid + i * NTHR;
+        const int c = p.colmode ? (e % TB) : (e / kL);
+        const int n = p.colmode ? (e / TB) : (e % kL);
+        cpx x = v[i];
+        if (cj_in) x.y = -x.y;
+        if (twid) x = cmul(x, stockham_root(p, int64_t(n) * cur_gq[c]));
+        data[c * kLP + pad16(n)] = x;
+      }
     }
     const int64_t next = tile + gridDim.x;
     int64_t* nxt = offs + (par ^ 1) * 2 * TB;
@@ -450,15 +480,18 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
     }
     if (!ok) break;
 
-    // ---- store the tile
+    // ---- store the tile: transform by transform where each transform's
+    // outputs are contiguous (rows, and the first pass of a Stockham chain),
+    // else adjacent threads on adjacent transforms
     {
       cpx* out = static_cast<cpx*>(p.out);
       const int nv = valid(tile);
+      const bool rows_out = !p.colmode || p.out_k == 1;
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int e = tid + i * NTHR;
-        const int c = p.colmode ? (e % TB) : (e / kL);
-        const int n = p.colmode ? (e / TB) : (e % kL);
+        const int c = rows_out ? (e / kL) : (e % TB);
+        const int n = rows_out ? (e % kL) : (e / TB);
         if (c < nv) {
           cpx x = cscale(data[c * kLP + pad16(n)], invs[c]);
           if (cj_out) x.y = -x.y;
