@@ -196,7 +196,9 @@ int minfft_b200_tune_set_default(int pipe, int cpb, int radix);
  * stay inside their buffers, launch shapes and shared memory are within
  * limits, and passes that cannot run in place do not.  Returns the number of
  * violations (0 = sound, -1 = bad arguments); `report` receives a
- * description, `launches` the launch count. */
+ * description of the first violations or, for a sound plan, the launches'
+ * labels in launch order, one per line (truncated to report_len);
+ * `launches` the launch count. */
 int minfft_b200_plan_selfcheck(int op, int d, const int *Ns, int howmany, int alias, char *report, int report_len,
                                int *launches);
 /* The same for a plan in arithmetic mode `precision` (MINFFT_B200_PREC_*). */

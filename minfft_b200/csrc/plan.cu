@@ -1873,7 +1873,8 @@ Extent launch_extent(const Launch& ln) {
 // launch: element ranges inside their buffers, complex/real views of the
 // user buffers, launch shapes, and no in-place use of the passes that
 // cannot run in place.  Returns the number of violations (0 = plan is
-// sound); a description of the first ones goes to `report`.
+// sound); a description of the first ones goes to `report`, or, for a
+// sound plan, the launches' labels in launch order, one per line.
 MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns, int howmany, int alias,
                                                    int precision, char* report, int report_len, int* launches) {
   const int fam = op_family(op);
@@ -1961,6 +1962,8 @@ MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns,
     }
   }
   if (launches) *launches = (int)prog.launches.size();
+  if (bad == 0)
+    for (const Launch& ln : prog.launches) rep += ln.label + "\n";
   if (report && report_len > 0) snprintf(report, report_len, "%s", rep.c_str());
   return bad;
 }

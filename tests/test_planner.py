@@ -4,6 +4,7 @@ pass in place that cannot run in place.  This is the host-side reading of
 the kernels' index arithmetic, done for every workload size before any of it
 runs on a GPU."""
 import itertools
+import re
 
 import numpy as np
 import pytest
@@ -128,6 +129,35 @@ def test_tensor_core_plans_are_in_bounds(dims, precision):
             assert bad == 0, f"{op} {dims} {precision} howmany={howmany} alias={alias}:\n{rep}"
             _, _, n32 = eng.plan_selfcheck(op, dims, howmany, alias)
             assert n == n32
+
+
+# (length, passes of its chain in a tensor-core mode: 256-point tensor-core
+# passes first, then the CUDA-core ones, with the same pass count as FP32)
+TC_CHAINS = [(1 << 16, ["tc:256", "tc:256"]), (1 << 20, ["tc:256", "cplx:4096"]),
+             (1 << 24, ["cplx:4096", "cplx:4096"]), (1 << 25, ["tc:256", "tc:256", "cplx:512"]),
+             (1 << 26, ["tc:256", "tc:256", "cplx:1024"]), (1 << 29, ["tc:256", "cplx:2048", "cplx:1024"])]
+
+
+def chain_passes(report):
+    out = []
+    for lab in report.splitlines():
+        m = re.search(r"(tc_pass|axis_pass|axis_pipe)<([a-z0-9+]+)?[^,]*,L=(\d+)", lab)
+        if m:
+            out.append(("tc" if m.group(1) == "tc_pass" else m.group(2)) + ":" + m.group(3))
+    return out
+
+
+@pytest.mark.parametrize("precision", ["tc_f16", "tc_bf16"])
+@pytest.mark.parametrize("n,passes", TC_CHAINS, ids=[str(n) for n, _ in TC_CHAINS])
+def test_tensor_core_chain_split(n, passes, precision):
+    """A long complex axis in a tensor-core mode is split into as many
+    256-point passes as its FP32 pass count allows, placed first."""
+    eng = minfft_b200.engine(True)
+    bad, rep, _ = eng.plan_selfcheck("dft", (n,), 1, False, precision=precision)
+    assert bad == 0, rep
+    assert chain_passes(rep) == passes, rep
+    bad, rep32, _ = eng.plan_selfcheck("dft", (n,), 1, False)
+    assert bad == 0 and len(chain_passes(rep32)) == len(passes) and "tc_pass" not in rep32, rep32
 
 
 def test_tensor_core_modes_need_the_single_library():
