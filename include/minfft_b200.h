@@ -143,7 +143,10 @@ int minfft_b200_mixed_items(const minfft_b200_mixed *m);
 void minfft_b200_mixed_free(minfft_b200_mixed *m);
 
 /* ----------------------------------------------- tensor-core precision */
-/* Arithmetic of plan `a`'s complex 256-point axis passes (single-precision
+/* Arithmetic of plan `a`'s complex 256-point axis passes, including the
+ * 256-point passes over HBM of an axis too long for one thread block (in a
+ * tensor-core mode such an axis is split into as many 256-point passes as
+ * its pass count allows: 2^26 = 256 x 256 x 1024) (single-precision
  * library; no counterpart in the reference, whose arithmetic is its
  * `minfft_real` type, minfft.h:14-31):
  *   MINFFT_B200_PREC_FP32     FP32 on the CUDA cores (default);
