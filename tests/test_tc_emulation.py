@@ -8,9 +8,11 @@ component of its input lies in [256, 512).  Per radix-16 stage, each row of
 multiplied by the split real 32 x 32 form of the 16-point DFT matrix, keeping
 the products Ai Bj with i + j < terms; the leading product and the
 corrections accumulate in FP32 separately and are added; the stage-1 result is
-twiddled in FP32, and the scale is undone at the end.  The model
-shows the scheme itself meets the 1e-6 relative-L2 bar with margin, so the GPU
-tests measure the kernel, not the method."""
+twiddled in FP32, and the scale is undone at the end.  A Stockham chain of
+two such passes over a 65536-point axis, the second pre-twiddled in FP32 with
+roots built from table roots and their products as the kernel builds them, is
+modelled too.  The model shows the scheme itself meets the 1e-6 relative-L2
+bar with margin, so the GPU tests measure the kernel, not the method."""
 import numpy as np
 import pytest
 
@@ -85,6 +87,72 @@ def test_split_scheme_meets_the_bar(fmt, spread):
     for i in range(x.shape[0]):
         ref = oracle.apply("dft", x[i].astype(np.complex128), (256,), single=False, kind=oracle.best_kind())
         assert rel_l2(got[i], ref) <= 3e-7, (fmt, i)
+
+
+def stockham_roots(lt):
+    """w_lt^g for every g < lt as the kernel forms it: the product, in FP32,
+    of a coarse root w_lt^(a << lo) and a fine root w_lt^c (c < 2^lo), both
+    correctly rounded to FP32."""
+    lo = (int(np.log2(lt)) + 1) // 2
+    w = lambda e: np.exp(-2j * np.pi * e / lt).astype(np.complex64)  # noqa: E731
+    g = np.arange(lt)
+    return (w((g >> lo) << lo) * w(g & ((1 << lo) - 1))).astype(np.complex64)
+
+
+def pretwiddles(lt, q):
+    """Pre-twiddles w_lt^(q*n), n < 256, of the sub-DFTs with span index q in
+    the second pass of a 256 x 256 chain, built as the tensor-core kernel
+    builds them in column mode: element n = n0 + 16 i of a thread takes
+    base * d4^(i >> 2) * d^(i & 3) with base = w^(n0 q), d = w^(16 q),
+    d4 = w^(64 q) table roots and d^2, d^3, d^8, d^12 as FP32 products."""
+    r = stockham_roots(lt)
+    out = np.empty((len(q), 256), np.complex64)
+    for n0 in range(16):
+        base, d1, d4 = r[(n0 * q) % lt], r[(16 * q) % lt], r[(64 * q) % lt]
+        d2 = (d1 * d1).astype(np.complex64)
+        pw = [np.ones_like(d1), d1, d2, (d2 * d1).astype(np.complex64)]
+        d8 = (d4 * d4).astype(np.complex64)
+        pw4 = [None, d4, d8, (d8 * d4).astype(np.complex64)]
+        for i in range(16):
+            w = base
+            if i >> 2:
+                w = (w * pw4[i >> 2]).astype(np.complex64)
+            if i & 3:
+                w = (w * pw[i & 3]).astype(np.complex64)
+            out[:, n0 + 16 * i] = w
+    return out
+
+
+@pytest.mark.parametrize("fmt", ["f16", "bf16"])
+def test_split_scheme_in_a_stockham_chain_meets_the_bar(fmt):
+    """A 65536-point DFT as the tensor-core mode plans it: two 256-point
+    passes, x[n + 256 m] -> Y[n, q] (DFT over m) -> pre-twiddle w^(q n) in
+    FP32 -> X[q + 256 k] (DFT over n), both passes in the split scheme."""
+    lt = 1 << 16
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal(lt) + 1j * rng.standard_normal(lt)
+    a = x.astype(np.complex64).reshape(256, 256)          # a[m, n] = x[n + 256 m]
+    y = tc256(np.ascontiguousarray(a.T), fmt)              # y[n, q]
+    q = np.arange(256)
+    yt = (y.T * pretwiddles(lt, q)).astype(np.complex64)  # yt[q, n]
+    z = tc256(yt, fmt)                                     # z[q, k] = X[q + 256 k]
+    got = z.T.reshape(lt)
+    ref = oracle.apply("dft", x.astype(np.complex128), (lt,), single=False, kind=oracle.best_kind())
+    assert rel_l2(got, ref) <= 5e-7, fmt
+
+
+def test_chain_pretwiddles_match_exact_roots():
+    """Each product-built pre-twiddle comes from six table roots and nine
+    FP32 products at most: measured 7.2 * 2^-24 worst case and 1.6 * 2^-24
+    RMS from the exact root, the size of the FP32 rounding of the data it
+    multiplies."""
+    lt = 1 << 16
+    q = np.arange(256)
+    got = pretwiddles(lt, q).astype(np.complex128)
+    ref = np.exp(-2j * np.pi * np.outer(q, np.arange(256)) / lt)
+    err = np.abs(got - ref)
+    assert err.max() <= 12 * 2.0 ** -24
+    assert np.sqrt(np.mean(err ** 2)) <= 2 * 2.0 ** -24
 
 
 def test_split_terms_reconstruct_fp32():
