@@ -62,6 +62,24 @@ def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(dist, x: float, device) -> float:
+    """The maximum of x over all ranks (x itself without a process group):
+    a multi-rank time is the slowest rank's."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gflops(flops_per_step: float, steps: int, world: int, seconds: float) -> float:
+    """Whole-job GFLOP/s: every rank runs `steps` steps of its own replica
+    (the same work), all timed by the slowest rank."""
+    return flops_per_step * steps * world / seconds / 1e9
+
+
 def peaks():
     try:
         with open(PEAKS_PATH) as f:
@@ -984,11 +1002,7 @@ def run_engine(args):
     if dist:
         dist.barrier()
     W.check_errors()
-    ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dist, start.elapsed_time(end), dev)
 
     # the same steps again with launch-level timing (an event pair around
     # every launch on the plan's stream): per-kernel durations for the
@@ -1008,7 +1022,7 @@ def run_engine(args):
     if hasattr(W, "set_streams"):
         W.set_streams(True)
     flops_step = W.flops_per_transform * W.ops_per_step
-    value = flops_step * args.steps * world / (ms / 1e3) / 1e9
+    value = job_gflops(flops_step, args.steps, world, ms / 1e3)
 
     # per-kernel statistics -> roofline of the dominant kernel
     stats = []
@@ -1082,13 +1096,9 @@ def run_engine(args):
         for _ in range(k_e2e):
             W.e2e_step()
         torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([el], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(dist, time.perf_counter() - t0, dev)
         W.check_errors()
-        e2e = {"value": round(flops_step * k_e2e * world / el / 1e9, 3), "unit": "GFLOP/s",
+        e2e = {"value": round(job_gflops(flops_step, k_e2e, world, el), 3), "unit": "GFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": k_e2e,
                "ms_per_step": round(1000 * el / k_e2e, 3)}
         floor = copy_floor_ms(h2d, d2h)
