@@ -434,7 +434,19 @@ class WorkloadBatch4096:
                 "inputs": "re/im i.i.d. uniform[-1,1), seed 1",
                 "l2": "inputs rotate over 4 sets of 64 MiB (256 MiB), larger than L2"}
 
-    cpu_sequences = None
+    cpu_sequences = (("dft", ("dft", "invdft"), False),)
+
+    @classmethod
+    def cpu_sample(cls, P):
+        return (f"the whole step: {cls.howmany} transforms forward then inverse, OpenMP over the batch on {P} "
+                f"threads, one plan per thread")
+
+    @classmethod
+    def cpu_measure(cls, kind, threads, warm, reps):
+        """The reference's batched case as its users run it: `omp for` over the
+        1024 transforms, one plan per thread (a minfft plan is not re-entrant)."""
+        t = cpu_run(kind, cls.cpu_sequences, (cls.n,), cls.howmany, threads, reps, warm)
+        return t, 5.0 * cls.n * math.log2(cls.n) * cls.howmany * 2 * reps
 
 
 class WorkloadMixed:
@@ -923,6 +935,9 @@ def _ref_config(W):
     if W.name == "3d256":
         return {"workload": "3-D complex DFT 256x256x256 c64, forward then inverse", "dims": list(W.dims),
                 "precision": "f32 (reference single-precision build)", "flops": "5*N*log2(N) per transform, N=2^24"}
+    if W.name == "batch4096":
+        return {"workload": "1024 x complex DFT N=4096 c128, forward then inverse", "n": W.n, "batch": W.howmany,
+                "precision": "f64 (reference double build)", "flops": "5*N*log2(N) per transform"}
     if W.name == "long1d_c64":
         return {"workload": "1-D complex DFT N=2^26 c64, forward then inverse", "dims": list(W.dims),
                 "precision": "f32 (reference single-precision build)", "flops": "5*N*log2(N) per transform, N=2^26"}
