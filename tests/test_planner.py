@@ -4,6 +4,7 @@ pass in place that cannot run in place.  This is the host-side reading of
 the kernels' index arithmetic, done for every workload size before any of it
 runs on a GPU."""
 import itertools
+import os
 import re
 
 import numpy as np
@@ -164,3 +165,36 @@ def test_tensor_core_modes_need_the_single_library():
     eng = minfft_b200.engine(False)
     bad, _, _ = eng.plan_selfcheck("dft", (256,), 1, False, precision="tc_f16")
     assert bad == -1
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+def test_tuning_table_file_round_trip(single):
+    """The autotuner's table saves to and loads from a text file: comment
+    lines and malformed lines are skipped, entries with a radix other than 8
+    or 16 are dropped, and a saved table reloads to the same entries.  Plans
+    stay sound with a loaded table whatever it holds (every tuned value is
+    checked against the launch's limits before use)."""
+    eng = minfft_b200.engine(single)
+    d = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "tune")  # git-ignored
+    os.makedirs(d, exist_ok=True)
+    tag = "f32" if single else "f64"
+    src, out = os.path.join(d, f"in_{tag}.txt"), os.path.join(d, f"out_{tag}.txt")
+    good = ["0 4096 0 0 1 1 1 1 1 0 1 8", "0 512 1 0 0 4100 1 1025 1025 1 4 16", "3 1024 0 0 1 2048 1 1 1 0 2 16",
+            "0 4096 0 0 1 8 1 1 1 0 100000 16"]
+    with open(src, "w") as f:
+        f.write("# a comment\n" + "\n".join(good) + "\nnot a line\n0 4096 0 0 1 1 1 1 1 0 1 4\n1 2 3\n")
+    try:
+        eng.tune_clear()
+        eng.tune_load(src)
+        assert eng.tune_size() == len(good)
+        eng.tune_save(out)
+        with open(out) as f:
+            saved = [ln.strip() for ln in f if ln.strip() and not ln.startswith("#")]
+        assert sorted(saved) == sorted(good)
+        for op, dims in (("dft", (4096,)), ("dft", (2048, 2048)), ("realdft", (2048, 2048)), ("dct2", (1024,))):
+            bad, rep, _ = eng.plan_selfcheck(op, dims, 1, False)
+            assert bad == 0, rep
+        eng.tune_clear()
+        assert eng.tune_size() == 0
+    finally:
+        eng.tune_clear()
