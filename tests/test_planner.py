@@ -172,8 +172,9 @@ def test_tuning_table_file_round_trip(single):
     """The autotuner's table saves to and loads from a text file: comment
     lines and malformed lines are skipped, entries with a radix other than 8
     or 16 are dropped, and a saved table reloads to the same entries.  Plans
-    stay sound with a loaded table whatever it holds (every tuned value is
-    checked against the launch's limits before use)."""
+    stay sound with a loaded table, also when an entry for one of their
+    launches holds values outside the launch's limits (every tuned value is
+    checked before use)."""
     eng = minfft_b200.engine(single)
     d = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "tune")  # git-ignored
     os.makedirs(d, exist_ok=True)
@@ -196,5 +197,23 @@ def test_tuning_table_file_round_trip(single):
             assert bad == 0, rep
         eng.tune_clear()
         assert eng.tune_size() == 0
+        # the key of the one 4096-point row launch (complex, L, row mode, no
+        # pre-twiddle, staged or not, batch 1, unit strides): a valid entry
+        # is used (the pipelined form), out-of-range values are refused at
+        # planning time and the planner's own choice stays
+        with open(src, "w") as f:
+            f.write("0 4096 0 0 0 1 1 1 1 1 1 16\n0 4096 0 0 1 1 1 1 1 1 1 16\n")
+        eng.tune_load(src)
+        bad, rep, _ = eng.plan_selfcheck("dft", (4096,), 1, False)
+        assert bad == 0 and rep.startswith("axis_pipe<cplx,L=4096,row>"), rep
+        for form, cpb, radix in ((0, 100000, 16), (1, 100000, 8), (0, 0, 16), (1, -5, 16), (0, 3, 8)):
+            with open(src, "w") as f:
+                for staged in (0, 1):
+                    f.write(f"0 4096 0 0 {staged} 1 1 1 1 {form} {cpb} {radix}\n")
+            eng.tune_clear()
+            eng.tune_load(src)
+            assert eng.tune_size() == 2
+            bad, rep, n = eng.plan_selfcheck("dft", (4096,), 1, False)
+            assert bad == 0 and n == 1 and rep.startswith("axis_pass<cplx,L=4096,row>"), (form, cpb, radix, rep)
     finally:
         eng.tune_clear()
