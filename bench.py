@@ -80,6 +80,43 @@ def job_gflops(flops_per_step: float, steps: int, world: int, seconds: float) ->
     return flops_per_step * steps * world / seconds / 1e9
 
 
+_input_cache = {}
+
+
+def uniform_c64(dims, seed):
+    """re/im i.i.d. uniform[-1,1) from numpy PCG64(seed), as complex64
+    (kept for the other precisions of the same workload)."""
+    key = (tuple(dims), seed)
+    if key not in _input_cache:
+        rng = np.random.default_rng(seed)
+        x = np.empty(dims, dtype=np.complex64)
+        x.real = rng.uniform(-1, 1, dims)
+        x.imag = rng.uniform(-1, 1, dims)
+        _input_cache[key] = x
+    return _input_cache[key]
+
+
+_oracle_cache = {}
+
+
+def oracle_kind_name():
+    import oracle
+
+    return {"reference": "reference minfft.c compiled from its sources, double",
+            "restatement": "C restatement of minfft.c, double"}[oracle.best_kind()]
+
+
+def oracle_dft(name, seed, x, dims):
+    """The checker (never the measured path): the FP64 oracle's forward DFT
+    of x upcast to complex128, cached per workload input."""
+    key = (name, seed, tuple(dims))
+    if key not in _oracle_cache:
+        import oracle
+
+        _oracle_cache[key] = oracle.apply("dft", x.astype(np.complex128), dims, single=False, kind=oracle.best_kind())
+    return _oracle_cache[key]
+
+
 def peaks():
     try:
         with open(PEAKS_PATH) as f:
@@ -322,9 +359,10 @@ class Workload2D(PerPrecisionStreams):
             pt("dct2", hx.data_ptr(), h["c"].data_ptr(), check=False)
             pt("dct3", h["c"].data_ptr(), h["x3"].data_ptr(), check=False)
 
-    def config(self):
+    @classmethod
+    def config(cls):
         return {"workload": "2-D realdft->invrealdft and dct2->dct3 round trips, 2048x2048, f64 and f32",
-                "dims": list(self.dims), "precisions": ["f64", "f32"], "transforms_per_step": 8,
+                "dims": list(cls.dims), "precisions": ["f64", "f32"], "transforms_per_step": 8,
                 "flops": "2.5*N*log2(N) per transform, N=2^22",
                 "inputs": "i.i.d. standard normal, numpy PCG64 seed 2",
                 "l2": "inputs rotate over 4 buffer sets (192 MiB of inputs; each step writes ~250 MB), "
@@ -428,9 +466,10 @@ class WorkloadBatch4096:
         plan.batch("dft", self.hx.data_ptr(), hy.data_ptr(), self.howmany)
         plan.batch("invdft", hy.data_ptr(), hz.data_ptr(), self.howmany)
 
-    def config(self):
-        return {"workload": "1024 x complex DFT N=4096 c128, forward then inverse", "n": self.n,
-                "batch": self.howmany, "flops": "5*N*log2(N) per transform",
+    @classmethod
+    def config(cls):
+        return {"workload": "1024 x complex DFT N=4096 c128, forward then inverse", "n": cls.n,
+                "batch": cls.howmany, "flops": "5*N*log2(N) per transform",
                 "inputs": "re/im i.i.d. uniform[-1,1), seed 1",
                 "l2": "inputs rotate over 4 sets of 64 MiB (256 MiB), larger than L2"}
 
@@ -576,14 +615,24 @@ class WorkloadMixed:
             self.eng.mixed_execute(handle, st.cuda_stream)
             self.h_out[i].copy_(pool[ni:], non_blocking=True)
 
-    def config(self):
+    @classmethod
+    def io_bytes(cls):
+        from minfft_b200 import shapes
+
+        tot = 0
+        for op, n in zip(*cls.job_list()):
+            ins, inc, outs, outc = shapes(op, (n,))
+            tot += 4 * (int(np.prod(ins)) * (2 if inc else 1) + int(np.prod(outs)) * (2 if outc else 1))
+        return tot
+
+    @classmethod
+    def config(cls):
+        b = cls.io_bytes()
         return {"workload": "20000 mixed 1-D transforms, one persistent graph-launched kernel",
-                "count": self.count, "log2n": "uniform integer 4..16", "kinds": list(self.kinds),
+                "count": cls.count, "log2n": "uniform integer 4..16", "kinds": list(cls.kinds),
                 "precision": "f32", "flops": "5*N*log2(N) dft, 2.5*N*log2(N) real-data kinds",
-                "inputs": "standard normal (torch generator seed 4)",
-                "bytes_in_out": self.in_bytes + self.out_bytes,
-                "l2": "inputs and outputs total ~%.1f GB, far beyond the 126 MB L2" % ((self.in_bytes + self.out_bytes)
-                                                                                   / 1e9)}
+                "inputs": "standard normal (torch generator seed 4)", "bytes_in_out": b,
+                "l2": "inputs and outputs total ~%.1f GB, far beyond the 126 MB L2" % (b / 1e9)}
 
     cpu_sequences = ()
 
@@ -596,6 +645,7 @@ class Workload3D256:
     name = "3d256"
     dims = (256, 256, 256)
     nsets = 3
+    seed = 3
     dtype = "f32"
     precision = "fp32"
 
@@ -607,28 +657,26 @@ class Workload3D256:
         self.flops_per_transform = 5.0 * n * math.log2(n)
         self.ops_per_step = 2
         self.eng = minfft_b200.engine(True)
-        rng = np.random.default_rng(3)
-        mk = lambda: torch.from_numpy((rng.standard_normal(self.dims) + 1j * rng.standard_normal(self.dims))  # noqa
-                                      .astype(np.complex64)).to(dev)
-        self.xs = [mk() for _ in range(self.nsets)]
+        self.xs = [torch.from_numpy(uniform_c64(self.dims, self.seed + i)).to(dev) for i in range(self.nsets)]
         self.y = torch.empty(self.dims, dtype=torch.complex64, device=dev)
         self.z = torch.empty(self.dims, dtype=torch.complex64, device=dev)
         self.plan = self._mkplan()
-        # accuracy of this precision against the double-precision engine on the same input
-        e64 = minfft_b200.engine(False)
-        p64 = e64.plan("dft", self.dims)
-        x64 = self.xs[0].to(torch.complex128)
-        y64 = torch.empty_like(x64)
-        p64("dft", x64.data_ptr(), y64.data_ptr())
         self.plan("dft", self.xs[0].data_ptr(), self.y.data_ptr())
         self.plan("invdft", self.y.data_ptr(), self.z.data_ptr())
         torch.cuda.synchronize()
         self.eng.tc_status(self.plan.aux)
-        self.err = float(torch.linalg.vector_norm(self.y.to(torch.complex128) - y64) / torch.linalg.vector_norm(y64))
-        self.roundtrip = float(torch.linalg.vector_norm(self.z.to(torch.complex128) / n - x64) /
-                               torch.linalg.vector_norm(x64))
-        p64.free()
-        del x64, y64
+        self.accuracy = self._accuracy(self.y.cpu().numpy(), self.z.cpu().numpy())
+
+    def _accuracy(self, y, z):
+        """Relative L2 error of the forward result against the FP64 oracle
+        (the reference compiled from its sources where available) on the same
+        input upcast, and of the round trip against the input."""
+        x = self.xs[0].cpu().numpy()
+        ref = oracle_dft(self.name, self.seed, x, self.dims)
+        err = float(np.linalg.norm((y.astype(np.complex128) - ref).ravel()) / np.linalg.norm(ref.ravel()))
+        n = int(np.prod(self.dims))
+        rt = float(np.linalg.norm((z.astype(np.complex128) / n - x).ravel()) / np.linalg.norm(x.ravel()))
+        return {"rel_l2_vs_fp64_oracle": err, "oracle": oracle_kind_name(), "roundtrip_rel_l2": rt}
 
     def _mkplan(self):
         plan = self.eng.plan("dft", self.dims)
@@ -671,12 +719,11 @@ class Workload3D256:
         plan("dft", self.hx.data_ptr(), hy.data_ptr(), check=False)
         plan("invdft", hy.data_ptr(), hz.data_ptr(), check=False)
 
-    def config(self):
-        return {"workload": "3-D complex DFT 256x256x256 c64, forward then inverse", "dims": list(self.dims),
-                "precision": self.precision,
-                "rel_l2_vs_f64_engine": self.err, "roundtrip_rel_l2": self.roundtrip,
-                "flops": "5*N*log2(N) per transform, N=2^24",
-                "inputs": "re/im i.i.d. standard normal, numpy PCG64 seed 3",
+    @classmethod
+    def config(cls):
+        return {"workload": "3-D complex DFT 256x256x256 c64, forward then inverse", "dims": list(cls.dims),
+                "precision": cls.precision, "flops": "5*N*log2(N) per transform, N=2^24",
+                "inputs": "re/im i.i.d. uniform[-1,1), numpy PCG64 seeds 3..5",
                 "l2": "inputs rotate over 3 sets of 128 MiB, larger than the 126 MB L2"}
 
     cpu_sequences = (("dft", ("dft", "invdft"), True),)
@@ -793,9 +840,10 @@ class WorkloadLong1D(PerPrecisionStreams):
             p4("dct4", hi["r"].data_ptr(), h["c"].data_ptr(), check=False)
             p4("dst4", hi["r"].data_ptr(), h["s"].data_ptr(), check=False)
 
-    def config(self):
+    @classmethod
+    def config(cls):
         return {"workload": "1-D dft 2^26 (c128, c64) + dct4/dst4 2^24 (f64, f32)",
-                "n_dft": self.n_dft, "n_t4": self.n_t4, "transforms_per_step": 6,
+                "n_dft": cls.n_dft, "n_t4": cls.n_t4, "transforms_per_step": 6,
                 "flops": "5*N*log2(N) dft, 2.5*N*log2(N) dct4/dst4",
                 "inputs": "standard normal (torch generator seed 5)",
                 "l2": "inputs rotate over 2 sets (1.5 GiB per set), far beyond the 126 MB L2",
@@ -829,13 +877,13 @@ class WorkloadLong1DC64(Workload3D256):
     name = "long1d_c64"
     dims = (1 << 26,)
     nsets = 3
+    seed = 5
 
-    def config(self):
-        return {"workload": "1-D complex DFT N=2^26 c64, forward then inverse", "dims": list(self.dims),
-                "precision": self.precision,
-                "rel_l2_vs_f64_engine": self.err, "roundtrip_rel_l2": self.roundtrip,
-                "flops": "5*N*log2(N) per transform, N=2^26",
-                "inputs": "re/im i.i.d. standard normal, numpy PCG64 seed 3",
+    @classmethod
+    def config(cls):
+        return {"workload": "1-D complex DFT N=2^26 c64, forward then inverse", "dims": list(cls.dims),
+                "precision": cls.precision, "flops": "5*N*log2(N) per transform, N=2^26",
+                "inputs": "re/im i.i.d. uniform[-1,1), numpy PCG64 seeds 5..7",
                 "l2": "inputs rotate over 3 sets of 512 MiB, larger than the 126 MB L2"}
 
     @classmethod
@@ -906,6 +954,8 @@ def run_reference(args):
     if rank != 0:
         return 0
     W = WORKLOADS[args.workload]
+    if hasattr(W, "precision"):
+        W.precision = args.precision
     if not hasattr(W, "cpu_measure"):
         print(json.dumps({"impl": "reference", "unavailable": f"no CPU reference defined for workload {W.name}"}))
         return 0
@@ -928,29 +978,232 @@ def run_reference(args):
 
 
 def _ref_config(W):
-    if W.name == "mixed20000":
-        return {"workload": "20000 mixed 1-D transforms", "count": W.count, "log2n": "uniform integer 4..16",
-                "kinds": list(W.kinds), "precision": "f32",
-                "flops": "5*N*log2(N) dft, 2.5*N*log2(N) real-data kinds"}
-    if W.name == "3d256":
-        return {"workload": "3-D complex DFT 256x256x256 c64, forward then inverse", "dims": list(W.dims),
-                "precision": "f32 (reference single-precision build)", "flops": "5*N*log2(N) per transform, N=2^24"}
-    if W.name == "batch4096":
-        return {"workload": "1024 x complex DFT N=4096 c128, forward then inverse", "n": W.n, "batch": W.howmany,
-                "precision": "f64 (reference double build)", "flops": "5*N*log2(N) per transform"}
-    if W.name == "long1d_c64":
-        return {"workload": "1-D complex DFT N=2^26 c64, forward then inverse", "dims": list(W.dims),
-                "precision": "f32 (reference single-precision build)", "flops": "5*N*log2(N) per transform, N=2^26"}
-    if W.name == "long1d":
-        return {"workload": "1-D dft 2^26 (c128, c64) + dct4/dst4 2^24 (f64, f32)", "n_dft": W.n_dft,
-                "n_t4": W.n_t4, "transforms_per_step": 6, "flops": "5*N*log2(N) dft, 2.5*N*log2(N) dct4/dst4"}
-    cfg = {"workload": "2-D realdft->invrealdft and dct2->dct3 round trips, 2048x2048, f64 and f32",
-           "dims": list(W.dims), "precisions": ["f64", "f32"], "transforms_per_step": 8,
-           "flops": "2.5*N*log2(N) per transform, N=2^22"}
-    return cfg
+    """The workload's config, identical to the engine arm's."""
+    return W.config()
 
 
 # ---------------------------------------------------------------- engine arm
+def copy_floor_ms(torch, dev, h2d_bytes, d2h_bytes, reps=5):
+    """Milliseconds to move one step's input bytes host->device and its
+    output bytes device->host at the same time (pinned host memory, one
+    stream per direction, no kernels): the transfer floor of an end-to-end
+    step."""
+    hi = torch.empty(max(int(h2d_bytes), 16), dtype=torch.uint8).pin_memory()
+    di = torch.empty(hi.numel(), dtype=torch.uint8, device=dev)
+    ho = torch.empty(max(int(d2h_bytes), 16), dtype=torch.uint8).pin_memory()
+    do = torch.empty(ho.numel(), dtype=torch.uint8, device=dev)
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def once():
+        with torch.cuda.stream(s_in):
+            di.copy_(hi, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            ho.copy_(do, non_blocking=True)
+
+    once()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(reps):
+        once()
+    torch.cuda.synchronize()
+    return 1000 * (time.perf_counter() - t) / reps
+
+
+def measure(torch, dev, dist, W, args, steps, warmup, e2e_seconds=5.0, cpu_seconds=10.0, cpu=True, e2e=True):
+    """Tune, time and profile workload W; returns the fields of its JSON line."""
+    rank, world, local = rank_info()
+    tuned = 0
+    tune_path = lambda eng: f"{args.tune_file}.{'f32' if eng.single else 'f64'}"  # noqa: E731
+    if args.tune_file and list(W.plans()) and all(os.path.exists(tune_path(e)) for e, _, _ in W.plans()):
+        # reuse a saved tuning table (e.g. for deterministic profiling runs)
+        for eng, plan, ops in W.plans():
+            eng.tune_load(tune_path(eng))
+            tuned = max(tuned, eng.tune_size())
+        for eng, plan, ops in list(W.plans()):
+            W.rebuild(eng, plan)
+    elif not args.no_tune:
+        # project autotuner: pick kernel form, radix and tile size per launch (setup, untimed)
+        for eng, plan, ops in W.plans():
+            for op in ops:
+                eng.autotune(plan.aux, op, getattr(W, "howmany_for", lambda o: 1)(op), 5)
+            tuned = max(tuned, eng.tune_size())
+        if hasattr(W, "tune"):
+            tuned = W.tune()
+        if args.tune_file:
+            for eng, plan, ops in W.plans():
+                eng.tune_save(tune_path(eng))
+    launches_per_step = W.launches_per_step()
+
+    # warm-up
+    for k in range(warmup):
+        W.step(k)
+    torch.cuda.synchronize()
+    W.check_errors()
+
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    side = W.step_streams() if hasattr(W, "step_streams") else []
+    with ClockSampler(local) as clocks:
+        start.record()
+        for st in side:  # workloads whose plans run on their own streams: fork ...
+            st.wait_event(start)
+        for k in range(steps):
+            W.step(k)
+        for st in side:  # ... and join before the end event
+            torch.cuda.current_stream().wait_stream(st)
+        end.record()
+        end.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    W.check_errors()
+    ms = max_over_ranks(dist, start.elapsed_time(end), dev)
+
+    # the same steps again with launch-level timing (an event pair around
+    # every launch on the plan's stream): per-kernel durations for the
+    # roofline.  The events serialise consecutive launches, so these
+    # durations are upper bounds and this pass is not the headline number.
+    # Plans that run concurrently in the timed loop are put on one stream
+    # here, so that each launch's duration is its own.
+    prof_steps = min(steps, 500)
+    if hasattr(W, "set_streams"):
+        W.set_streams(False)
+    for eng, plan, ops in W.plans():
+        eng.profile(plan.aux, prof_steps * 8 + 64)
+    torch.cuda.synchronize()
+    for k in range(prof_steps):
+        W.step(k)
+    torch.cuda.synchronize()
+    if hasattr(W, "set_streams"):
+        W.set_streams(True)
+    flops_step = W.flops_per_transform * W.ops_per_step
+    value = job_gflops(flops_step, steps, world, ms / 1e3)
+
+    # per-kernel statistics -> roofline of the dominant kernel
+    stats = []
+    for eng, plan, ops in W.plans():
+        prec = "f32" if eng.single else "f64"
+        for lab, cnt, tot, by in eng.profile_stats(plan.aux):
+            stats.append((f"{prec} {lab}", cnt, tot, by))
+        eng.profile(plan.aux, 0)
+    if not stats and hasattr(W, "roofline_stats"):
+        stats = W.roofline_stats(ms, steps)  # one launch per step: the timed region itself
+    stats.sort(key=lambda r: -r[2])
+    hbm, peak_src = peaks()
+    roof = None
+    if stats:
+        lab, cnt, tot, by = stats[0]
+        avg_ms = tot / cnt
+        achieved = by / (avg_ms / 1e3) / 1e9
+        traffic = None
+        try:
+            with open(TRAFFIC_PATH) as f:
+                traffic = json.load(f).get(W.name, {}).get(lab)
+        except Exception:
+            traffic = None
+        roof = {"bound": "hbm", "kernel": lab, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": by, "avg_launch_us": round(avg_ms * 1e3, 2),
+                "traffic": traffic}
+    kernel_table = [{"kernel": lab, "launches": cnt, "total_ms": round(tot, 3),
+                     "share": round(tot / sum(s[2] for s in stats), 4),
+                     "gbs": round(by / (tot / cnt / 1e3) / 1e9, 1)} for lab, cnt, tot, by in stats]
+
+    # end to end through the C ABI with pinned host buffers
+    e2e_rec = None
+    if e2e and not args.no_e2e:
+        h2d, d2h = W.e2e_setup()
+        W.e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        W.e2e_step()
+        torch.cuda.synchronize()
+        est = time.perf_counter() - t0
+        k_e2e = max(3, min(steps, int(e2e_seconds / max(est, 1e-4))))
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            W.e2e_step()
+        torch.cuda.synchronize()
+        el = max_over_ranks(dist, time.perf_counter() - t0, dev)
+        W.check_errors()
+        e2e_rec = {"value": round(job_gflops(flops_step, k_e2e, world, el), 3), "unit": "GFLOP/s",
+                   "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": k_e2e,
+                   "ms_per_step": round(1000 * el / k_e2e, 3)}
+        floor = copy_floor_ms(torch, dev, h2d, d2h)
+        e2e_rec["copy_floor_ms_per_step"] = round(floor, 3)
+        e2e_rec["frac_of_copy_floor"] = round(floor / (1000 * el / k_e2e), 4)
+
+    # CPU baseline (rank 0, one GPU only): the reference on the host cores
+    cpu_rec = None
+    if cpu and rank == 0 and world == 1 and not args.no_cpu and hasattr(W, "cpu_measure"):
+        cpu_rec = cpu_baseline(W, cpu_seconds)
+
+    rec = {"value": round(value, 3), "ms_per_step": round(ms / steps, 4), "steps": steps, "warmup": warmup,
+           "dtype": W.dtype, "config": W.config(), "gpu_launches": int(launches_per_step * steps),
+           "clocks": clocks.summary(), "autotuned_launch_configs": tuned, "roofline": roof, "e2e": e2e_rec,
+           "cpu_baseline": cpu_rec, "kernels": kernel_table[:8]}
+    if getattr(W, "accuracy", None):
+        rec["accuracy"] = W.accuracy
+    return rec
+
+
+def cpu_baseline(W, seconds):
+    """The reference library on all host cores for workload W: one sample,
+    repeated up to about `seconds` of CPU work."""
+    P = cpu_threads()
+    kind = cpu_kind()
+    reps = 1
+    t, flops = W.cpu_measure(kind, P, 1, reps)
+    if t < seconds / 2:
+        reps = min(100, int(math.ceil(seconds / max(t, 1e-3))))
+        t, flops = W.cpu_measure(kind, P, 1, reps)
+    return {"value": round(flops / t / 1e9, 3), "unit": "GFLOP/s", "cores": P, "kind": kind,
+            "sample": (W.cpu_sample(P) if hasattr(W, "cpu_sample") else
+                       f"{P} concurrent independent instances of one step (one per OpenMP thread, own plans)")
+            + f", {reps} timed repetition(s), {t:.1f} s"}
+
+
+# Every other workload of the benchmark, measured briefly after the headline
+# (one GPU only): (label, workload, precision).
+SUB_CONFIGS = (("batch4096", "batch4096", None),
+               ("3d256_fp32", "3d256", "fp32"), ("3d256_tc_f16", "3d256", "tc_f16"),
+               ("3d256_tc_bf16", "3d256", "tc_bf16"),
+               ("mixed20000", "mixed20000", None),
+               ("long1d", "long1d", None),
+               ("long1d_c64_fp32", "long1d_c64", "fp32"), ("long1d_c64_tc_f16", "long1d_c64", "tc_f16"),
+               ("long1d_c64_tc_bf16", "long1d_c64", "tc_bf16"))
+
+
+def single_thread_reference():
+    """Seconds per call of the reference on ONE host thread for the
+    single-transform workloads (2048^2 real/trig, 256^3 complex, 2^26 complex
+    and 2^24 type-4): one untimed and one timed call each."""
+    out = {}
+    kind = cpu_kind()
+    cases = (("2d2048 realdft f64", "realdft", ("realdft",), (2048, 2048), False),
+             ("2d2048 invrealdft f64", "realdft", ("invrealdft",), (2048, 2048), False),
+             ("2d2048 dct2 f64", "t2t3", ("dct2",), (2048, 2048), False),
+             ("2d2048 dct3 f64", "t2t3", ("dct3",), (2048, 2048), False),
+             ("2d2048 realdft f32", "realdft", ("realdft",), (2048, 2048), True),
+             ("2d2048 dct2 f32", "t2t3", ("dct2",), (2048, 2048), True),
+             ("3d256 dft c64", "dft", ("dft",), (256, 256, 256), True),
+             ("long1d dft 2^26 c128", "dft", ("dft",), (1 << 26,), False),
+             ("long1d dft 2^26 c64", "dft", ("dft",), (1 << 26,), True),
+             ("long1d dct4 2^24 f64", "t4", ("dct4",), (1 << 24,), False),
+             ("long1d dct4 2^24 f32", "t4", ("dct4",), (1 << 24,), True))
+    for label, fam, ops, dims, single in cases:
+        t = cpu_run(kind, ((fam, ops, single),), dims, 1, 1, 1, 1)
+        n = int(np.prod(dims))
+        f = (5.0 if fam == "dft" else 2.5) * n * math.log2(n)
+        out[label] = {"ms_per_call": round(1000 * t, 2), "gflops": round(f / t / 1e9, 3)}
+    return {"kind": kind, "threads": 1, "calls": out}
+
+
 def run_engine(args):
     import torch
 
@@ -969,181 +1222,59 @@ def run_engine(args):
     if hasattr(WC, "precision"):
         WC.precision = args.precision
     W = WC(torch, dev)
-    tuned = 0
-    tune_path = lambda eng: f"{args.tune_file}.{'f32' if eng.single else 'f64'}"  # noqa: E731
-    if args.tune_file and list(W.plans()) and all(os.path.exists(tune_path(e)) for e, _, _ in W.plans()):
-        # reuse a saved tuning table (e.g. for deterministic profiling runs)
-        for eng, plan, ops in W.plans():
-            eng.tune_load(f"{args.tune_file}.{'f32' if eng.single else 'f64'}")
-            tuned = max(tuned, eng.tune_size())
-        for eng, plan, ops in W.plans():
-            W.rebuild(eng, plan)
-    elif not args.no_tune:
-        # project autotuner: pick kernel form, radix and tile size per launch (setup, untimed)
-        for eng, plan, ops in W.plans():
-            for op in ops:
-                eng.autotune(plan.aux, op, getattr(W, "howmany_for", lambda o: 1)(op), 5)
-            tuned = max(tuned, eng.tune_size())
-        if hasattr(W, "tune"):
-            tuned = W.tune()
-        if args.tune_file:
-            for eng, plan, ops in W.plans():
-                eng.tune_save(f"{args.tune_file}.{'f32' if eng.single else 'f64'}")
-    launches_per_step = W.launches_per_step()
-
-    # warm-up
-    for k in range(args.warmup):
-        W.step(k)
+    rec = measure(torch, dev, dist, W, args, args.steps, args.warmup)
+    del W
     torch.cuda.synchronize()
-    W.check_errors()
+    torch.cuda.empty_cache()
 
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    side = W.step_streams() if hasattr(W, "step_streams") else []
-    with ClockSampler(local) as clocks:
-        start.record()
-        for st in side:  # workloads whose plans run on their own streams: fork ...
-            st.wait_event(start)
-        for k in range(args.steps):
-            W.step(k)
-        for st in side:  # ... and join before the end event
-            torch.cuda.current_stream().wait_stream(st)
-        end.record()
-        end.synchronize()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    W.check_errors()
-    ms = max_over_ranks(dist, start.elapsed_time(end), dev)
-
-    # the same steps again with launch-level timing (an event pair around
-    # every launch on the plan's stream): per-kernel durations for the
-    # roofline.  The events serialise consecutive launches, so these
-    # durations are upper bounds and this pass is not the headline number.
-    # Plans that run concurrently in the timed loop are put on one stream
-    # here, so that each launch's duration is its own.
-    prof_steps = min(args.steps, 500)
-    if hasattr(W, "set_streams"):
-        W.set_streams(False)
-    for eng, plan, ops in W.plans():
-        eng.profile(plan.aux, prof_steps * 8 + 64)
-    torch.cuda.synchronize()
-    for k in range(prof_steps):
-        W.step(k)
-    torch.cuda.synchronize()
-    if hasattr(W, "set_streams"):
-        W.set_streams(True)
-    flops_step = W.flops_per_transform * W.ops_per_step
-    value = job_gflops(flops_step, args.steps, world, ms / 1e3)
-
-    # per-kernel statistics -> roofline of the dominant kernel
-    stats = []
-    for eng, plan, ops in W.plans():
-        prec = "f32" if eng.single else "f64"
-        for lab, cnt, tot, by in eng.profile_stats(plan.aux):
-            stats.append((f"{prec} {lab}", cnt, tot, by))
-        eng.profile(plan.aux, 0)
-    if not stats and hasattr(W, "roofline_stats"):
-        stats = W.roofline_stats(ms, args.steps)  # one launch per step: the timed region itself
-    stats.sort(key=lambda r: -r[2])
-    hbm, peak_src = peaks()
-    roof = None
-    if stats:
-        lab, cnt, tot, by = stats[0]
-        avg_ms = tot / cnt
-        achieved = by / (avg_ms / 1e3) / 1e9
-        traffic = None
-        try:
-            with open(TRAFFIC_PATH) as f:
-                traffic = json.load(f).get(args.workload, {}).get(lab)
-        except Exception:
-            traffic = None
-        roof = {"bound": "hbm", "kernel": lab, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(achieved / hbm, 4), "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": by, "avg_launch_us": round(avg_ms * 1e3, 2),
-                "traffic": traffic}
-    kernel_table = [{"kernel": lab, "launches": cnt, "total_ms": round(tot, 3),
-                     "share": round(tot / sum(s[2] for s in stats), 4),
-                     "gbs": round(by / (tot / cnt / 1e3) / 1e9, 1)} for lab, cnt, tot, by in stats]
-
-    # end to end through the C ABI with pinned host buffers
-    def copy_floor_ms(h2d_bytes, d2h_bytes, reps=5):
-        """Milliseconds to move one step's input bytes host->device and its
-        output bytes device->host at the same time (pinned host memory, one
-        stream per direction, no kernels): the transfer floor of an
-        end-to-end step."""
-        hi = torch.empty(max(int(h2d_bytes), 16), dtype=torch.uint8).pin_memory()
-        di = torch.empty(hi.numel(), dtype=torch.uint8, device=dev)
-        ho = torch.empty(max(int(d2h_bytes), 16), dtype=torch.uint8).pin_memory()
-        do = torch.empty(ho.numel(), dtype=torch.uint8, device=dev)
-        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
-
-        def once():
-            with torch.cuda.stream(s_in):
-                di.copy_(hi, non_blocking=True)
-            with torch.cuda.stream(s_out):
-                ho.copy_(do, non_blocking=True)
-
-        once()
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        for _ in range(reps):
-            once()
-        torch.cuda.synchronize()
-        return 1000 * (time.perf_counter() - t) / reps
-
-    e2e = None
-    if not args.no_e2e:
-        h2d, d2h = W.e2e_setup()
-        W.e2e_step()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        W.e2e_step()
-        torch.cuda.synchronize()
-        est = time.perf_counter() - t0
-        k_e2e = max(3, min(args.steps, int(5.0 / max(est, 1e-4))))
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(k_e2e):
-            W.e2e_step()
-        torch.cuda.synchronize()
-        el = max_over_ranks(dist, time.perf_counter() - t0, dev)
-        W.check_errors()
-        e2e = {"value": round(job_gflops(flops_step, k_e2e, world, el), 3), "unit": "GFLOP/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": k_e2e,
-               "ms_per_step": round(1000 * el / k_e2e, 3)}
-        floor = copy_floor_ms(h2d, d2h)
-        e2e["copy_floor_ms_per_step"] = round(floor, 3)
-        e2e["frac_of_copy_floor"] = round(floor / (1000 * el / k_e2e), 4)
-
-    # CPU baseline (rank 0, one GPU only): the reference on the host cores
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu and hasattr(W, "cpu_measure"):
-        P = cpu_threads()
-        kind = cpu_kind()
-        reps = 1
-        t, flops = W.cpu_measure(kind, P, 1, reps)
-        if t < 5.0:  # a short sample: repeat it to about 10 s of CPU work
-            reps = min(100, int(math.ceil(10.0 / max(t, 1e-3))))
-            t, flops = W.cpu_measure(kind, P, 1, reps)
-        cpu = {"value": round(flops / t / 1e9, 3), "unit": "GFLOP/s", "cores": P, "kind": kind,
-               "sample": (W.cpu_sample(P) if hasattr(W, "cpu_sample") else
-                          f"{P} concurrent independent instances of one step (one per OpenMP thread, own plans)")
-               + f", {reps} timed repetition(s), {t:.1f} s"}
+    configs = None
+    single_ref = None
+    if world == 1 and not args.no_configs and args.workload == "2d2048" and args.precision == "fp32":
+        configs = {}
+        base_vals = {}
+        for label, wname, prec in SUB_CONFIGS:
+            WS = WORKLOADS[wname]
+            if prec is not None:
+                WS.precision = prec
+            w = WS(torch, dev)
+            r = measure(torch, dev, None, w, args, args.sub_steps, 3, e2e_seconds=1.0, cpu_seconds=3.0,
+                        cpu=(prec in (None, "fp32")))
+            entry = {"value": r["value"], "ms_per_step": r["ms_per_step"], "steps": r["steps"],
+                     "config": r["config"], "dtype": r["dtype"], "gpu_launches": r["gpu_launches"],
+                     "roofline_frac": r["roofline"]["frac"] if r["roofline"] else None,
+                     "top_kernel": r["roofline"]["kernel"] if r["roofline"] else None,
+                     "top_kernel_gbs": r["roofline"]["achieved"] if r["roofline"] else None,
+                     "e2e": r["e2e"], "reference_cpu": r["cpu_baseline"], "clocks": r["clocks"]}
+            if "accuracy" in r:
+                entry["accuracy"] = r["accuracy"]
+            if prec == "fp32":
+                base_vals[wname] = r["value"]
+            elif prec is not None and wname in base_vals:
+                entry["tc_vs_fp32"] = round(r["value"] / base_vals[wname], 4)
+            configs[label] = entry
+            del w
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+        WC.precision = args.precision
+        if not args.no_cpu:
+            single_ref = single_thread_reference()
 
     if rank == 0:
-        line = {"metric": "GFLOP/s (5N log2N complex, 2.5N log2N real-data)", "value": round(value, 3),
+        line = {"metric": "GFLOP/s (5N log2N complex, 2.5N log2N real-data)", "value": rec["value"],
                 "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": W.dtype,
-                "data": "synthetic", "config": W.config(), "parallelism": f"replicas x{world}",
-                "gpu_launches": int(launches_per_step * args.steps), "clocks": clocks.summary(),
-                "autotuned_launch_configs": tuned,
-                "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "kernels": kernel_table[:8]}
+                "ms_per_step": rec["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": rec["dtype"],
+                "data": "synthetic", "config": rec["config"], "parallelism": f"replicas x{world}",
+                "gpu_launches": rec["gpu_launches"], "clocks": rec["clocks"],
+                "autotuned_launch_configs": rec["autotuned_launch_configs"],
+                "roofline": rec["roofline"], "e2e": rec["e2e"], "cpu_baseline": rec["cpu_baseline"],
+                "kernels": rec["kernels"]}
+        if "accuracy" in rec:
+            line["accuracy"] = rec["accuracy"]
+        if configs is not None:
+            line["configs"] = configs
+        if single_ref is not None:
+            line["reference_single_thread"] = single_ref
         print(json.dumps(line))
     if dist:
         dist.barrier()
@@ -1162,6 +1293,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (heuristic launch configurations)")
     ap.add_argument("--tune-file", default="", help="tuning table prefix: loaded if present, else saved after tuning")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the short runs of the other workloads after the default headline")
+    ap.add_argument("--sub-steps", type=int, default=10, help="timed steps of each other workload")
     ap.add_argument("--precision", choices=["fp32", "tc_f16", "tc_bf16"], default="fp32",
                     help="3d256, long1d_c64: arithmetic of the 256-point axis passes")
     args = ap.parse_args()

@@ -208,6 +208,26 @@ int minfft_b200_plan_selfcheck(int op, int d, const int *Ns, int howmany, int al
 int minfft_b200_plan_selfcheck_precision(int op, int d, const int *Ns, int howmany, int alias, int precision,
                                          char *report, int report_len, int *launches);
 
+/* ------------------------------------------------------------ test hooks */
+/* Failure injection for tests of the allocation paths (no counterpart in the
+ * reference, whose makers call malloc directly, minfft.c:1024-1054).  With
+ * k > 0, the k-th device allocation the library attempts after this call
+ * fails as cudaMalloc does when device memory is short (nothing is
+ * allocated for it); k = 0 turns injection off.  Either way the allocation
+ * counter restarts at 0.  Process-wide; meant for single-threaded tests. */
+int minfft_b200_test_fail_device_alloc(long long k);
+/* Device allocations attempted since the last
+ * minfft_b200_test_fail_device_alloc call (or since the library loaded). */
+long long minfft_b200_test_device_alloc_count(void);
+/* Timeout injection for the tensor-core pass (no counterpart in the
+ * reference, which has no device waits).  With polls > 0, every tensor-core
+ * launch issued afterwards withholds the matrix operations of its first
+ * stage, so that stage's completion wait -- limited to `polls` polls -- runs
+ * out: the launch leaves its output incomplete and records the timeout for
+ * minfft_b200_device_status (MINFFT_B200_ETIMEOUT).  polls = 0 restores
+ * normal launches.  No fault is involved; meant for tests. */
+int minfft_b200_test_tc_withhold(long long polls);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

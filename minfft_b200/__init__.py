@@ -114,6 +114,12 @@ class Engine(MinfftLibrary):
         L.minfft_b200_mixed_items.restype = i32
         L.minfft_b200_mixed_free.argtypes = [vp]
         L.minfft_b200_mixed_free.restype = None
+        L.minfft_b200_test_fail_device_alloc.argtypes = [i64]
+        L.minfft_b200_test_fail_device_alloc.restype = i32
+        L.minfft_b200_test_device_alloc_count.argtypes = []
+        L.minfft_b200_test_device_alloc_count.restype = i64
+        L.minfft_b200_test_tc_withhold.argtypes = [i64]
+        L.minfft_b200_test_tc_withhold.restype = i32
 
     # --------------------------------------------------------- errors
     def last_error(self) -> int:

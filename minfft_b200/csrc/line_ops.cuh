@@ -43,8 +43,7 @@ __device__ __forceinline__ ItemIdx split_item(int64_t e, int64_t inner, int64_t 
 // complex t_m = (u_2m, u_2m+1) of the type-2 permutation (see LoadDCT2)
 struct Op_dct2_pre {
   static __device__ __forceinline__ int64_t count(const LineParams& p) {
-    const int64_t L = p.L, N = 2 * L;
-    const real sg = (p.flags & F_DST) ? real(-1) : real(1);
+    const int64_t L = p.L;
     return p.outer * p.inner * L;
   }
   static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
@@ -62,8 +61,7 @@ struct Op_dct2_pre {
 // type-4 pre-rotation (see LoadT4)
 struct Op_t4_pre {
   static __device__ __forceinline__ int64_t count(const LineParams& p) {
-    const int64_t L = p.L, N = 2 * L;
-    const bool dst = (p.flags & F_DST) != 0;
+    const int64_t L = p.L;
     return p.outer * p.inner * L;
   }
   static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
@@ -115,7 +113,6 @@ struct Op_c2r_pack {
 struct Op_dct3_pack {
   static __device__ __forceinline__ int64_t count(const LineParams& p) {
     const int64_t L = p.L, K = L / 2 + 1;
-    const bool dst = (p.flags & F_DST) != 0;
     return p.outer * p.inner * K;
   }
   static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
@@ -172,9 +169,6 @@ struct Op_r2c_unpack {
 struct Op_dct2_post {
   static __device__ __forceinline__ int64_t count(const LineParams& p) {
     const int64_t L = p.L, K = L / 2 + 1;
-    const int N = int(2 * L);
-    const bool dst = (p.flags & F_DST) != 0;
-    const real r2 = real(1.414213562373095048801688724209698079);
     return p.outer * p.inner * K;
   }
   static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
@@ -205,8 +199,7 @@ struct Op_dct2_post {
 // type-3 de-interleave of the conjugated forward result (see StoreDCT3)
 struct Op_dct3_post {
   static __device__ __forceinline__ int64_t count(const LineParams& p) {
-    const int64_t L = p.L, N = 2 * L;
-    const bool dst = (p.flags & F_DST) != 0;
+    const int64_t L = p.L;
     return p.outer * p.inner * L;
   }
   static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
@@ -226,8 +219,7 @@ struct Op_dct3_post {
 // type-4 post-rotation (see StoreT4)
 struct Op_t4_post {
   static __device__ __forceinline__ int64_t count(const LineParams& p) {
-    const int64_t L = p.L, N = 2 * L;
-    const bool dst = (p.flags & F_DST) != 0;
+    const int64_t L = p.L;
     return p.outer * p.inner * L;
   }
   static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {

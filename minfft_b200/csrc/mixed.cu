@@ -40,6 +40,11 @@
 namespace mb {
 void set_last_error(int code, const char* msg);
 void host_table(int kind, int64_t N, std::vector<cpx>& h);
+cudaError_t dev_malloc(void** p, size_t bytes);  // every device allocation of the library (plan.cu)
+template <class T>
+cudaError_t dev_malloc(T** p, size_t bytes) {
+  return dev_malloc(reinterpret_cast<void**>(p), bytes);
+}
 }  // namespace mb
 
 namespace mb {
@@ -456,7 +461,7 @@ const cpx* upload(minfft_b200_mixed* m, int kind, int64_t N) {
   std::vector<cpx> h;
   mb::host_table(kind, N, h);
   void* d = nullptr;
-  if (!ok(cudaMalloc(&d, h.size() * sizeof(cpx)), "cudaMalloc(table)")) return nullptr;
+  if (!ok(mb::dev_malloc(&d, h.size() * sizeof(cpx)), "cudaMalloc(table)")) return nullptr;
   m->tables.push_back(d);
   if (!ok(cudaMemcpy(d, h.data(), h.size() * sizeof(cpx), cudaMemcpyHostToDevice), "cudaMemcpy(table)"))
     return nullptr;
@@ -514,8 +519,8 @@ bool build_items(minfft_b200_mixed* m) {
   if (m->d_order) cudaFree(m->d_order);
   if (m->d_items) cudaFree(m->d_items);
   m->d_order = m->d_items = nullptr;
-  if (!ok(cudaMalloc(&m->d_order, std::max<size_t>(1, m->order.size()) * sizeof(int)), "cudaMalloc(order)") ||
-      !ok(cudaMalloc(&m->d_items, std::max<size_t>(1, m->items.size()) * sizeof(Item)), "cudaMalloc(items)"))
+  if (!ok(mb::dev_malloc(&m->d_order, std::max<size_t>(1, m->order.size()) * sizeof(int)), "cudaMalloc(order)") ||
+      !ok(mb::dev_malloc(&m->d_items, std::max<size_t>(1, m->items.size()) * sizeof(Item)), "cudaMalloc(items)"))
     return false;
   if (!m->order.empty() &&
       !ok(cudaMemcpy(m->d_order, m->order.data(), m->order.size() * sizeof(int), cudaMemcpyHostToDevice),
@@ -650,13 +655,13 @@ MB_EXPORT minfft_b200_mixed* minfft_b200_mixed_plan(int count, const minfft_b200
               "occupancy query");
   m->per_sm = std::max(1, occ);
   m->grid = sms * m->per_sm;
-  if (good) good = ok(cudaMalloc(&m->d_jobs, count * sizeof(Job)), "cudaMalloc(jobs)");
+  if (good) good = ok(mb::dev_malloc(&m->d_jobs, count * sizeof(Job)), "cudaMalloc(jobs)");
   if (good)
     good = ok(cudaMemcpy(m->d_jobs, m->jobs.data(), count * sizeof(Job), cudaMemcpyHostToDevice), "cudaMemcpy(jobs)");
-  if (good) good = ok(cudaMalloc(&m->d_counter, sizeof(unsigned)), "cudaMalloc(counter)");
+  if (good) good = ok(mb::dev_malloc(&m->d_counter, sizeof(unsigned)), "cudaMalloc(counter)");
   if (good && max_big > 0) {
     P.scratch_stride = int64_t(2) << kBigMaxLog2L;
-    good = ok(cudaMalloc(&m->d_scratch, size_t(m->grid) * P.scratch_stride * sizeof(cpx)), "cudaMalloc(scratch)");
+    good = ok(mb::dev_malloc(&m->d_scratch, size_t(m->grid) * P.scratch_stride * sizeof(cpx)), "cudaMalloc(scratch)");
   }
   P.jobs = static_cast<const Job*>(m->d_jobs);
   P.counter = m->d_counter;

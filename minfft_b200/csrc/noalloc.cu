@@ -26,7 +26,11 @@
 //
 // Set-up.  The first call on each device looks up the arrays' device
 // addresses (cudaGetSymbolAddress, once per device, with that device
-// current); issue that first call before any stream capture.
+// current); issue that first call before any stream capture.  The lookup is
+// tied to the device's context: after cudaDeviceReset the module is loaded
+// again (its arrays may move), so the next call on that device, which sees a
+// new context, repeats the set-up.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -59,23 +63,57 @@ static __device__ __align__(256) cpx g_noalloc_roots[4 * kRootSlot];
 struct DeviceArrays {
   cpx* scratch = nullptr;
   cpx* roots = nullptr;
+  unsigned long long ctx_id = 0;  // the context the addresses belong to
 };
 
 std::mutex g_mu;
 DeviceArrays g_arrays[128];
 
-// Device addresses of the static arrays on `dev` (looked up once per device).
+// Unique id of the calling thread's current context (the device's primary
+// context once the runtime has set it up); a reset device gets a new one.
+// The driver functions come through the runtime, so the library does not
+// link libcuda itself.
+bool current_context_id(unsigned long long* id) {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    return cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess
+               ? reinterpret_cast<GetCurrent>(f)
+               : nullptr;
+  }();
+  static GetId get_id = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    return cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess
+               ? reinterpret_cast<GetId>(f)
+               : nullptr;
+  }();
+  CUcontext ctx = nullptr;
+  return get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Device addresses of the static arrays on `dev`, looked up once per device
+// (again after the device's context changed, e.g. after cudaDeviceReset).
+// The caller has already made a runtime call on `dev` (the pointer checks),
+// so its primary context is current.
 bool device_arrays(int dev, DeviceArrays* out) {
   if (dev < 0 || dev >= 128) return false;
+  unsigned long long id = 0;
+  if (!current_context_id(&id)) return false;
   std::lock_guard<std::mutex> lk(g_mu);
   DeviceArrays& a = g_arrays[dev];
-  if (!a.scratch) {
+  if (!a.scratch || a.ctx_id != id) {
     cpx* s = nullptr;
     cpx* r = nullptr;
     if (cudaGetSymbolAddress((void**)&s, g_noalloc_scratch) != cudaSuccess) return false;
     if (cudaGetSymbolAddress((void**)&r, g_noalloc_roots) != cudaSuccess) return false;
     a.scratch = s;
     a.roots = r;
+    a.ctx_id = id;
   }
   *out = a;
   return true;
@@ -123,6 +161,8 @@ MB_EXPORT int minfft_b200_dft_noalloc(const void* x, void* y, int n, int inverse
   if (!x || !y) return fail(MINFFT_B200_EINVAL, "minfft_b200_dft_noalloc: NULL data pointer");
   if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % sizeof(cpx) != 0)
     return fail(MINFFT_B200_EINVAL, "minfft_b200_dft_noalloc: complex data must be aligned to its size");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(MINFFT_B200_ECUDA, "minfft_b200_dft_noalloc: no device");
   for (const void* p : {x, static_cast<const void*>(y)}) {
     cudaPointerAttributes attr;
     if (cudaPointerGetAttributes(&attr, p) != cudaSuccess ||
@@ -130,9 +170,9 @@ MB_EXPORT int minfft_b200_dft_noalloc(const void* x, void* y, int n, int inverse
       cudaGetLastError();
       return fail(MINFFT_B200_EINVAL, "minfft_b200_dft_noalloc: x and y must be device memory");
     }
+    if (attr.type == cudaMemoryTypeDevice && attr.device != dev)
+      return fail(MINFFT_B200_EINVAL, "minfft_b200_dft_noalloc: x and y must be on the current device");
   }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return fail(MINFFT_B200_ECUDA, "minfft_b200_dft_noalloc: no device");
   DeviceArrays arr;
   if (!device_arrays(dev, &arr))
     return fail(MINFFT_B200_ECUDA, "minfft_b200_dft_noalloc: cudaGetSymbolAddress failed");

@@ -22,6 +22,7 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -77,6 +78,32 @@ bool cuda_ok(cudaError_t e, const char* what) {
             cudaGetErrorString(e));
   return false;
 }
+
+// Failure injection for the allocation paths (a test hook, off by default):
+// when g_fail_at = k > 0, the k-th device allocation counted from the call
+// that set it fails as cudaMalloc does when memory is short.
+std::atomic<long long> g_alloc_count{0};
+std::atomic<long long> g_fail_at{0};
+// Test hook: > 0 makes tensor-core launches withhold their first commit and
+// give up after this many polls (see mb::TcParams).
+std::atomic<long long> g_tc_withhold{0};
+
+}  // namespace
+
+namespace mb {
+// Every device allocation of the library goes through here.
+cudaError_t dev_malloc(void** p, size_t bytes) {
+  const long long n = ++g_alloc_count;
+  const long long k = g_fail_at.load();
+  if (k > 0 && n == k) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+}  // namespace mb
+
+namespace {
 
 // ========================================================== unit roots
 // (cos, sin)(2*pi*n/N), with the angle folded into [0, pi/4] before calling
@@ -371,7 +398,7 @@ const cpx* table(minfft_aux* a, int kind, int64_t N) {
   if (h.empty()) return nullptr;
   void* d = nullptr;
   const size_t bytes = h.size() * sizeof(cpx);
-  if (!cuda_ok(cudaMalloc(&d, bytes), "cudaMalloc(table)")) return nullptr;
+  if (!cuda_ok(mb::dev_malloc(&d, bytes), "cudaMalloc(table)")) return nullptr;
   if (!cuda_ok(cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice), "cudaMemcpy(table)")) {
     cudaFree(d);
     return nullptr;
@@ -1075,7 +1102,6 @@ struct Planner {
     // --- the HBM passes
     int prev = cs;
     int64_t Ns = 1;
-    int last_src = cs;
     int cd = s.out_buf;
     for (int p = 0; p < P; ++p) {
       const int64_t Rp = int64_t(1) << pb[p];
@@ -1120,11 +1146,9 @@ struct Planner {
       ap.tw = tab(TB_TW, Rp);
       add_axis_kernel(mb::K_CPLX, (int)Rp, outer * (Lp / Rp), ap, prev, dst, false, false);
       if (ok) prog->launches.back().hbm_pass = true;
-      last_src = prev;
       prev = dst;
       Ns *= Rp;
     }
-    (void)last_src;
 
     // --- post-processing
     if (post) {
@@ -1307,7 +1331,7 @@ bool ensure_buffer(minfft_aux* a, int buf, size_t bytes) {
   a->bufs[buf] = nullptr;
   a->buf_bytes[buf] = 0;
   void* p = nullptr;
-  if (!cuda_ok(cudaMalloc(&p, bytes), "cudaMalloc(scratch)")) return false;
+  if (!cuda_ok(mb::dev_malloc(&p, bytes), "cudaMalloc(scratch)")) return false;
   a->bufs[buf] = p;
   a->buf_bytes[buf] = bytes;
   return true;
@@ -1398,6 +1422,11 @@ bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
   }
   if (ln.tc) {
     mb::TcParams tcp = ln.tcp;
+    const long long withhold = g_tc_withhold.load();
+    if (withhold > 0) {
+      tcp.withhold = 1;
+      tcp.wait_polls = withhold;
+    }
     void* targs[2] = {&ap, &tcp};
     return enqueue(a, ln, targs, ln.smem, "launch(tc)");
   }
@@ -1470,7 +1499,7 @@ bool grow(void** p, size_t* have, size_t want) {
   if (*p) cudaFree(*p);
   *p = nullptr;
   *have = 0;
-  if (!cuda_ok(cudaMalloc(p, want), "cudaMalloc(staging)")) return false;
+  if (!cuda_ok(mb::dev_malloc(p, want), "cudaMalloc(staging)")) return false;
   *have = want;
   return true;
 }
@@ -1560,7 +1589,7 @@ minfft_aux* make_plan(int family, int d, const int* Ns) {
   }
   {
     void* st = nullptr;
-    if (!cuda_ok(cudaMalloc(&st, 16), "cudaMalloc(status)") || !cuda_ok(cudaMemset(st, 0, 16), "cudaMemset(status)")) {
+    if (!cuda_ok(mb::dev_malloc(&st, 16), "cudaMalloc(status)") || !cuda_ok(cudaMemset(st, 0, 16), "cudaMemset(status)")) {
       if (st) cudaFree(st);
       delete a;
       return nullptr;
@@ -1713,7 +1742,7 @@ MB_EXPORT int minfft_b200_set_precision(minfft_aux* a, int mode) {
     img.insert(img.end(), img2.begin(), img2.end());
     img.resize(img.size() + 8, 0);
     void* d = nullptr;
-    if (!cuda_ok(cudaMalloc(&d, b16 + bb + 16), "cudaMalloc(tc operands)")) return g_err;
+    if (!cuda_ok(mb::dev_malloc(&d, b16 + bb + 16), "cudaMalloc(tc operands)")) return g_err;
     if (!cuda_ok(cudaMemcpy(d, img.data(), b16 + bb + 16, cudaMemcpyHostToDevice), "cudaMemcpy(tc operands)")) {
       cudaFree(d);
       return g_err;
@@ -2151,5 +2180,28 @@ MB_EXPORT int minfft_b200_tune_size(void) {
 MB_EXPORT int minfft_b200_tune_set_default(int pipe, int cpb, int radix) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_default_override = TuneVal{pipe < 0 ? -1 : (pipe ? 1 : 0), cpb < 0 ? 0 : cpb, radix == 8 ? 8 : 16};
+  return MINFFT_B200_OK;
+}
+
+// ------------------------------------------------------------ test hooks
+MB_EXPORT int minfft_b200_test_fail_device_alloc(long long k) {
+  if (k < 0) {
+    set_error(MINFFT_B200_EINVAL, "allocation index must be >= 0");
+    return MINFFT_B200_EINVAL;
+  }
+  g_fail_at.store(0);
+  g_alloc_count.store(0);
+  g_fail_at.store(k);
+  return MINFFT_B200_OK;
+}
+
+MB_EXPORT long long minfft_b200_test_device_alloc_count(void) { return g_alloc_count.load(); }
+
+MB_EXPORT int minfft_b200_test_tc_withhold(long long polls) {
+  if (polls < 0) {
+    set_error(MINFFT_B200_EINVAL, "poll count must be >= 0");
+    return MINFFT_B200_EINVAL;
+  }
+  g_tc_withhold.store(polls);
   return MINFFT_B200_OK;
 }

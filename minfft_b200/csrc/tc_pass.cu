@@ -184,8 +184,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&d)[16]) {
       : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-  for (long long i = 0; i < kSpinLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, long long limit = kSpinLimit) {
+  for (long long i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
@@ -295,7 +295,10 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
   const int grp = tid >> 7, row = tid & 127;  // UMMA group and row of this thread's sub-DFT
   const int t = tid >> 4, dgt = tid & 15;     // its transform and digit
   bool ok = true;
+  bool pending = false;  // MMAs committed and not yet waited for
+  bool first = true;     // the first stage of this CTA (test hook: withheld)
   uint32_t phase = 0;
+  const long long first_limit = q.wait_polls > 0 ? q.wait_polls : kSpinLimit;
 
   cpx v[16];
   auto valid = [&](int64_t tl) {
@@ -412,7 +415,8 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
       // ---- the MMAs, two K steps of 16 each: per group, the corrections
       // Ai Bj (0 < i + j < NT, smallest first) into columns 64g+32.., then
       // the leading A0 B0 into columns 64g..
-      if (tid == 0) {
+      const bool withheld = first && q.withhold;
+      if (tid == 0 && !withheld) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
         for (int g = 0; g < G; ++g) {
@@ -440,12 +444,15 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_a)
                      : "memory");
       }
-      if (!mbar_wait(mbar_a, phase)) atomicExch(bad, 1);
+      pending = !withheld;
+      if (!mbar_wait(mbar_a, phase, first ? first_limit : kSpinLimit)) atomicExch(bad, 1);
+      first = false;
       __syncthreads();
       if (*bad) {
         ok = false;
         break;
       }
+      pending = false;
       phase ^= 1;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       // ---- this row of D: columns 0..15 Re y_k, 16..31 Im y_k of both
@@ -505,8 +512,9 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
   if (!ok) {
     if (tid == 0 && q.status) atomicExch(q.status, 1);
     // the MMAs of the abandoned stage may still be running: give them one
-    // more bounded wait before the columns are released
-    mbar_wait(mbar_a, phase);
+    // more bounded wait (the full limit) before the columns are released;
+    // a stage that committed nothing has nothing to wait for
+    if (pending) mbar_wait(mbar_a, phase);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

@@ -19,6 +19,12 @@ enum TcFormat : int {
 struct TcParams {
   const void* bmat;  // split DFT-16 operands, tc_bmat_bytes(fmt) bytes (tc_bmat_host)
   int* status;       // set to 1 when a CTA gave up waiting for its tensor-core work
+  // Test hook (zero in normal launches): with withhold = 1 the first stage
+  // of each CTA's first tile issues no MMA and no commit, so its wait -- limited
+  // to wait_polls polls -- runs out and the status path is exercised without
+  // any fault.
+  long long wait_polls;
+  int withhold;
 };
 
 constexpr int kTcLength = 256;

@@ -89,3 +89,26 @@ def apply(op: str, x: np.ndarray, dims: Sequence[int], single: bool = False, kin
     finally:
         lib.free(aux)
     return y
+
+
+def apply_rows(op: str, rows, n: int, single: bool = False, kind: Optional[str] = None):
+    """Run 1-D transform ``op`` of length ``n`` on every array in ``rows``
+    with one plan (the reference's plans serve any number of calls); returns
+    the list of outputs."""
+    kind = kind or "restatement"
+    lib = library(kind, single)
+    in_shape, in_cplx, out_shape, out_cplx = shapes(op, (n,))
+    rdt, cdt = np_dtypes(single)
+    aux = lib.mkaux(OP_FAMILY[op], (n,))
+    if not aux:
+        raise ValueError(f"plan maker returned NULL for {op} ({n},)")
+    outs = []
+    try:
+        for x in rows:
+            xin = np.ascontiguousarray(x, dtype=cdt if in_cplx else rdt).reshape(in_shape).copy()
+            y = np.zeros(out_shape, dtype=cdt if out_cplx else rdt)
+            lib.run(op, xin.ctypes.data, y.ctypes.data, aux)
+            outs.append(y)
+    finally:
+        lib.free(aux)
+    return outs

@@ -5,9 +5,11 @@ is owned by another allocator's pool or a fixed budget, or an allocation's
 latency and implied synchronisation are unacceptable in their loop -- and so
 cannot hold a plan.  These tests call it through the C ABI and check that it
 agrees with the planned entry point (minfft_mkaux_dft_1d + minfft_dft /
-minfft_invdft) within the parity tolerance, on two calls in a row (the calls
-share the static scratch array, so the second must not see stale state), and
-that lengths beyond its fixed maximum are refused with an error.
+minfft_invdft) and with the double-precision oracle within the parity
+tolerance, on two calls in a row (the calls share the static scratch array,
+so the second must not see stale state), that a call takes no device memory,
+and that lengths beyond its fixed maximum, host memory and another device's
+memory are refused with an error.
 
 This file sorts last so that a run stopping at the first failure has run
 every other test first; it also passes alone in a fresh process.
@@ -18,6 +20,7 @@ import numpy as np
 import pytest
 
 import minfft_b200
+import oracle
 from conftest import rel_l2, tolerance
 
 torch = pytest.importorskip("torch")
@@ -60,6 +63,37 @@ def test_noalloc_matches_planned_dft_on_consecutive_calls(single):
         ref = planned(eng, x, inverse)
         err = rel_l2(y.cpu().numpy(), ref.cpu().numpy())
         assert err <= tolerance(single, (n,)), (n, inverse, err)
+        # and against the oracle on the same (upcast) input
+        want = oracle.apply("invdft" if inverse else "dft", x.cpu().numpy().astype(np.complex128), (n,),
+                            kind=oracle.best_kind())
+        err = rel_l2(y.cpu().numpy(), want)
+        assert err <= tolerance(single, (n,)), (n, inverse, err)
+
+
+def test_noalloc_takes_no_device_memory():
+    eng = minfft_b200.engine(False)
+    f = noalloc_fn(eng)
+    x = torch.randn(MAX_N, dtype=torch.complex128, device="cuda")
+    y = torch.empty_like(x)
+    assert f(x.data_ptr(), y.data_ptr(), MAX_N, 0, None) == 0  # first call: set-up on this device
+    torch.cuda.synchronize()
+    before_torch = torch.cuda.memory_allocated()
+    before_free = torch.cuda.mem_get_info()[0]
+    for inverse in (0, 1):
+        assert f(x.data_ptr(), y.data_ptr(), MAX_N, inverse, None) == 0, eng.last_error_message()
+    torch.cuda.synchronize()
+    assert torch.cuda.memory_allocated() == before_torch
+    assert torch.cuda.mem_get_info()[0] == before_free
+
+
+@pytest.mark.skipif(not torch.cuda.is_available() or torch.cuda.device_count() < 2, reason="needs two devices")
+def test_noalloc_refuses_another_devices_memory():
+    eng = minfft_b200.engine(False)
+    f = noalloc_fn(eng)
+    torch.cuda.set_device(0)
+    other = torch.zeros(64, dtype=torch.complex128, device="cuda:1")
+    assert f(other.data_ptr(), other.data_ptr(), 64, 0, None) == 1  # MINFFT_B200_EINVAL, nothing launched
+    assert "current device" in eng.last_error_message()
 
 
 @pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
