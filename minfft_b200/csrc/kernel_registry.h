@@ -27,6 +27,10 @@ const void* axis_kernel(int combo, int log2L, int R = 16);
 // for log2(L) = 1 .. 13, or nullptr.
 const void* pipe_kernel(int combo, int log2L, int R = 16);
 
+// The streamed complex column pass (stream_pass.cuh) for log2(L) = 4 .. 9 and
+// radix R (16, or 8 where the CTA stays within 512 threads), or nullptr.
+const void* stream_kernel(int log2L, int R);
+
 // Root tables kept on the device by plans: w_N^m (m < N); the real-DFT
 // table w_N^k (k < N/4); the type-2/3 table w_4N^n (n < N/2); the type-4
 // tables w_2N^n (n < N/2) and w_8N^(2q+1) (q < N); and the coarse/fine pair

@@ -37,6 +37,7 @@
 #include "axis_pass.cuh"
 #include "kernel_registry.h"
 #include "pipe_pass.cuh"
+#include "stream_pass.cuh"
 #include "line_kernels.h"
 #include "tc_pass.h"
 #include "minfft.h"
@@ -253,6 +254,9 @@ struct Launch {
   bool out_c = false;    // the kernel writes its output as complex values
   bool hbm_pass = false; // a pass of the Stockham FFT over HBM (never in place)
   bool pipe = false;     // persistent pipelined kernel (pipe_pass.cuh)
+  bool stream = false;   // persistent TMA-fed column pass (stream_pass.cuh)
+  int tcs = 0;           // tensor-core pass in streamed form: 1 column tiles, 2 row tiles
+  int64_t st_d2 = 1;     // streamed pass: outermost batch extent of its tensor copies
   bool tc = false;       // tensor-core split-precision pass (tc_pass.cu)
   mb::TcParams tcp{};    // its B operands and status word
   int ch_static = 16;    // pipelined kernel: copy chunk allowed by the strides
@@ -523,8 +527,113 @@ struct Planner {
     return pb;
   }
 
+  // Form of the tensor-core pass: the streamed form (tc_stream_kernel) by
+  // default, the one-tile form with MINFFT_B200_TC_FORM=tile; stages of the
+  // streamed form from MINFFT_B200_TC_STAGES (2 .. 6, default 3).
+  static bool tc_stream_default() {
+    static const bool on = [] {
+      const char* e = getenv("MINFFT_B200_TC_FORM");
+      return !(e && strcmp(e, "tile") == 0);
+    }();
+    return on;
+  }
+  static int tc_stream_stages() {
+    static const int n = [] {
+      const char* e = getenv("MINFFT_B200_TC_STAGES");
+      const int v = e ? atoi(e) : 3;
+      return v < 2 ? 2 : (v > 6 ? 6 : v);
+    }();
+    return n;
+  }
+
+  // Normalised layout of the streamed tensor-core pass: b0 indexes the
+  // transforms of a tile (adjacent columns at unit stride, or rows of
+  // contiguous points), d0 * d1 divides the batch.
+  static bool tc_stream_normalise(int64_t nbatch, AxisParams& ap) {
+    if (ap.d0 == 1 && ap.d1 > 1) {
+      const int64_t d1 = ap.d1;
+      ap.d0 = d1;
+      ap.is0 = ap.is1;
+      ap.os0 = ap.os1;
+      ap.d1 = (nbatch + d1 - 1) / d1;
+      ap.is1 = ap.is2;
+      ap.os1 = ap.os2;
+      ap.is2 = 0;
+      ap.os2 = 0;
+    }
+    if (ap.d0 < 2 || nbatch % (ap.d0 * ap.d1) != 0) return false;
+    return ap.colmode ? ap.is0 == 1 : ap.in_n == 1;
+  }
+
+  bool add_tc_stream_kernel(int fmt, int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf,
+                            const TuneKey& key) {
+    if (!tc_stream_default() || L != mb::kTcLength || !tc_stream_normalise(nbatch, ap)) return false;
+    if (!ap.colmode && (ap.flags & mb::F_STAGE_ROWS)) return false;
+    const bool rows = !ap.colmode;
+    const int stages = tc_stream_stages();
+    Launch ln;
+    ln.key = key;
+    ln.radix = 16;
+    ln.tc = true;
+    ln.tcs = rows ? 2 : 1;
+    ln.fn = mb::tc_stream_kernel_fn(fmt, rows);
+    if (!ln.fn) return false;
+    ln.smem = mb::tc_stream_smem(fmt, stages);
+    if (ln.smem > (size_t)dev_max_smem) return false;
+    if (!a->host_only && !ensure_smem_attr(ln.fn, ln.smem)) {
+      ok = false;
+      return true;
+    }
+    if (a->host_only) {
+      static uint4 dummy[1];
+      ln.tcp.bmat = dummy;
+      ln.tcp.status = nullptr;
+    } else {
+      if (!a->tc_mem) {
+        set_error(MINFFT_B200_EINVAL, "tensor-core operands missing (set the precision first)");
+        ok = false;
+        return true;
+      }
+      ln.tcp.bmat = static_cast<const char*>(a->tc_mem) + (fmt == mb::TC_F16 ? 0 : mb::tc_bmat_bytes(mb::TC_F16));
+      ln.tcp.status = a->dev_status;
+    }
+    const int W = mb::kTcStreamTile;
+    ap.nbatch = nbatch;
+    ap.cpb = stages;
+    ap.stage_bytes = mb::tc_stream_stage_bytes();
+    ap.gpb = (ap.d0 + W - 1) / W;
+    ln.st_d2 = nbatch / (ap.d0 * ap.d1);
+    ap.ntiles = ap.gpb * ap.d1 * ln.st_d2;
+    ap.lp = 0;
+    ln.block = unsigned(mb::kTcStreamThreads);
+    int occ = 1;
+    if (!a->host_only) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ln.fn, (int)ln.block, ln.smem) != cudaSuccess ||
+          occ < 1) {
+        cudaGetLastError();
+        occ = 1;
+      }
+      occ = std::min(occ, 512 / 128);  // tensor memory: 128 columns per CTA
+    }
+    ln.grid = unsigned(std::min<int64_t>(ap.ntiles, int64_t(sms) * occ));
+    ln.in_buf = in_buf;
+    ln.out_buf = out_buf;
+    ln.in_c = ln.out_c = true;
+    ln.combo = mb::K_CPLX;
+    ln.L = L;
+    ln.ap = ap;
+    ln.bytes = 2.0 * L * sizeof(cpx) * double(nbatch);
+    char buf[160];
+    snprintf(buf, sizeof(buf), "tc_stream<%s,L=%d,%s> batch=%lld", fmt == mb::TC_F16 ? "f16x3" : "bf16x6", L,
+             rows ? "row" : "col", (long long)nbatch);
+    ln.label = buf;
+    prog->launches.push_back(ln);
+    return true;
+  }
+
   void add_tc_kernel(int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, const TuneKey& key) {
     const int fmt = a->precision == MINFFT_B200_PREC_TC_BF16 ? mb::TC_BF16 : mb::TC_F16;
+    if (add_tc_stream_kernel(fmt, L, nbatch, ap, in_buf, out_buf, key)) return;
     const int tb = ap.colmode ? 16 : 8;  // column mode: 16 adjacent columns = 128-byte runs
     Launch ln;
     ln.key = key;
@@ -612,7 +721,11 @@ struct Planner {
     TuneVal tv;
     int R = 16;  // per-thread radix of the one-tile-per-CTA form
     if (tune_lookup(key, &tv)) {
-      if (tv.pipe && pipe_fits(combo, L, tv.cpb, ap.colmode, tv.radix)) {
+      if (tv.pipe == 2 && stream_fits(combo, L, nbatch, ap, tv.radix, tv.cpb)) {
+        add_stream_kernel(L, nbatch, ap, in_buf, out_buf, tv.cpb, key, tv.radix);
+        return;
+      }
+      if (tv.pipe == 1 && pipe_fits(combo, L, tv.cpb, ap.colmode, tv.radix)) {
         add_pipe_kernel(combo, L, nbatch, ap, in_buf, out_buf, tv.cpb, key, tv.radix);
         return;
       }
@@ -627,6 +740,11 @@ struct Planner {
         ov = g_default_override;
       }
       const bool want_pipe = ov.pipe == 1 || (ov.pipe < 0 && pipe_default());
+      const int st_stages = ov.cpb > 0 ? ov.cpb : 3;
+      if (ov.pipe == 2 && stream_fits(combo, L, nbatch, ap, ov.radix, st_stages)) {
+        add_stream_kernel(L, nbatch, ap, in_buf, out_buf, st_stages, key, ov.radix);
+        return;
+      }
       if (want_pipe) {
         int pc = ov.cpb > 0 ? ov.cpb : choose_pipe_cpb(combo, L, ap.colmode != 0);
         const int rr = pipe_fits(combo, L, 1, ap.colmode, ov.radix) ? ov.radix : 16;
@@ -718,6 +836,86 @@ struct Planner {
     auto smem = [&](int c) { return mb::pipe_smem(L, R, c, colmode ? 1 : 0, er, esz); };
     while (cpb > 1 && smem(cpb) > (size_t)dev_max_smem) cpb /= 2;
     return cpb;
+  }
+
+  // The streamed column pass covers complex column-mode launches whose
+  // adjacent transforms are adjacent in the input (the batch index of unit
+  // input stride is the innermost one, possibly after dropping a unit d0),
+  // lengths 16 .. 512 and `stages` tiles of shared memory in flight.  It
+  // rewrites `ap` into that normalised form.
+  bool stream_normalise(int combo, int L, int64_t nbatch, AxisParams& ap) const {
+    if (combo != mb::K_CPLX || !ap.colmode || L < 16 || L > 512) return false;
+    if (ap.d0 == 1 && ap.d1 > 1) {
+      // b = b1 + d1*b2: the transforms of unit stride are the b1 ones
+      const int64_t d1 = ap.d1;
+      ap.d0 = d1;
+      ap.is0 = ap.is1;
+      ap.os0 = ap.os1;
+      ap.d1 = (nbatch + d1 - 1) / d1;
+      ap.is1 = ap.is2;
+      ap.os1 = ap.os2;
+      ap.is2 = 0;
+      ap.os2 = 0;
+    }
+    if (ap.is0 != 1 || ap.d0 < 2 || nbatch % (ap.d0 * ap.d1) != 0) return false;
+    return true;
+  }
+
+  bool stream_fits(int combo, int L, int64_t nbatch, const AxisParams& ap0, int R, int stages) const {
+    AxisParams ap = ap0;
+    if (!stream_normalise(combo, L, nbatch, ap)) return false;
+    if (stages < 2 || stages > 8 || !mb::stream_kernel(ilog2(L), R)) return false;
+    return mb::stream_smem(L, stages) <= (size_t)dev_max_smem;
+  }
+
+  void add_stream_kernel(int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, int stages,
+                         const TuneKey& key, int R) {
+    stream_normalise(mb::K_CPLX, L, nbatch, ap);
+    const int W = mb::stream_cols();
+    Launch ln;
+    ln.key = key;
+    ln.radix = R;
+    ln.fn = mb::stream_kernel(ilog2(L), R);
+    ln.stream = true;
+    ap.nbatch = nbatch;
+    ap.cpb = stages;
+    ap.stage_bytes = mb::stream_stage_bytes(L);
+    ap.gpb = (ap.d0 + W - 1) / W;
+    ln.st_d2 = nbatch / (ap.d0 * ap.d1);
+    ap.ntiles = ap.gpb * ap.d1 * ln.st_d2;
+    ap.lp = 0;
+    ln.smem = mb::stream_smem(L, stages);
+    if (!ln.fn || ln.smem > (size_t)dev_max_smem) {
+      set_error(MINFFT_B200_EUNSUPPORTED, "no streamed pass for L=%d with %d stages", L, stages);
+      ok = false;
+      return;
+    }
+    if (!a->host_only && !ensure_smem_attr(ln.fn, ln.smem)) {
+      ok = false;
+      return;
+    }
+    ln.block = unsigned(W * (L / R));
+    int occ = 1;
+    if (!a->host_only) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ln.fn, (int)ln.block, ln.smem) != cudaSuccess ||
+          occ < 1) {
+        cudaGetLastError();
+        occ = 1;
+      }
+    }
+    ln.grid = unsigned(std::min<int64_t>(ap.ntiles, int64_t(sms) * occ));
+    ln.in_buf = in_buf;
+    ln.out_buf = out_buf;
+    ln.in_c = ln.out_c = true;
+    ln.combo = mb::K_CPLX;
+    ln.L = L;
+    ln.ap = ap;
+    ln.bytes = 2.0 * L * sizeof(cpx) * double(nbatch);
+    char buf[160];
+    snprintf(buf, sizeof(buf), "stream_pass<cplx,L=%d,col%s> batch=%lld", L, ap.st_ns > 1 ? ",hbm" : "",
+             (long long)nbatch);
+    ln.label = buf;
+    prog->launches.push_back(ln);
   }
 
   void add_pipe_kernel(int combo, int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, int cpb,
@@ -929,8 +1127,17 @@ struct Planner {
 
   // Forward: rows X -> block layout in `mid` (row j of block q at (q*Q + j)*K),
   // then length-Q column DFTs mid -> Y (output p of block q at row q + 4p).
+  // Row pitch of the intermediate of a split 2-D real DFT: K complex values
+  // rounded up to whole 16-byte units, so that its columns can be fetched
+  // with tensor copies (the extra column is never read).
+  static int64_t split_pitch(int64_t K) {
+    const int64_t per16 = int64_t(16 / sizeof(cpx));
+    return (K + per16 - 1) / per16 * per16;
+  }
+
   void plan_realdft_split(int64_t H, int64_t Nr, int64_t N, int in_buf, int mid, int out_buf) {
-    const int64_t K = N / 2 + 1, Q = Nr / 4, L = N / 2;
+    const int64_t K = N / 2 + 1, Q = Nr / 4, L = N / 2, Kp = split_pitch(K);
+    need(mid, size_t(H * Nr * Kp) * sizeof(cpx));
     AxisParams ap = base_params();
     ap.d0 = 4;
     ap.d1 = Q;
@@ -938,9 +1145,9 @@ struct Planner {
     ap.is1 = N;
     ap.is2 = Nr * N;
     ap.in_n = 1;
-    ap.os0 = Q * K;
-    ap.os1 = K;
-    ap.os2 = Nr * K;
+    ap.os0 = Q * Kp;
+    ap.os1 = Kp;
+    ap.os2 = Nr * Kp;
     ap.out_k = 1;
     ap.cpb = 4;
     ap.tw = tab(TB_TW, L);
@@ -951,9 +1158,9 @@ struct Planner {
     cp.d0 = K;
     cp.d1 = 4;
     cp.is0 = 1;
-    cp.is1 = Q * K;
-    cp.is2 = Nr * K;
-    cp.in_n = K;
+    cp.is1 = Q * Kp;
+    cp.is2 = Nr * Kp;
+    cp.in_n = Kp;
     cp.os0 = 1;
     cp.os1 = K;
     cp.os2 = Nr * K;
@@ -968,7 +1175,8 @@ struct Planner {
   // `mid`, then the fused radix-4 stage and the inverse real DFTs of the rows,
   // mid -> Y.
   void plan_invrealdft_split(int64_t H, int64_t Nr, int64_t N, int in_buf, int mid, int out_buf) {
-    const int64_t K = N / 2 + 1, Q = Nr / 4, L = N / 2;
+    const int64_t K = N / 2 + 1, Q = Nr / 4, L = N / 2, Kp = split_pitch(K);
+    need(mid, size_t(H * Nr * Kp) * sizeof(cpx));
     AxisParams cp = base_params();
     cp.d0 = K;
     cp.d1 = 4;
@@ -977,9 +1185,9 @@ struct Planner {
     cp.is2 = Nr * K;
     cp.in_n = 4 * K;
     cp.os0 = 1;
-    cp.os1 = Q * K;
-    cp.os2 = Nr * K;
-    cp.out_k = K;
+    cp.os1 = Q * Kp;
+    cp.os2 = Nr * Kp;
+    cp.out_k = Kp;
     cp.colmode = 1;
     cp.flags = mb::F_CONJ_IN | mb::F_CONJ_OUT;
     cp.cpb = choose_cpb(int(Q), true);
@@ -988,9 +1196,9 @@ struct Planner {
     AxisParams ap = base_params();
     ap.d0 = 4;
     ap.d1 = Q;
-    ap.is0 = Q * K;
-    ap.is1 = K;
-    ap.is2 = Nr * K;
+    ap.is0 = Q * Kp;
+    ap.is1 = Kp;
+    ap.is2 = Nr * Kp;
     ap.in_n = 1;
     ap.os0 = Q * N;
     ap.os1 = N;
@@ -1400,6 +1608,82 @@ bool enqueue(minfft_aux* a, const Launch& ln, void** args, size_t smem, const ch
 }
 
 // Enqueue one planned launch with its buffers resolved.
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links only the runtime).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return EncodeTiledFn(nullptr);
+    }
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  return fn;
+}
+
+// Tensor map of a streamed pass's input: dims (2*d0 reals, L elements, d1,
+// d2), box (2W reals, min(L, 256) elements, 1, 1).  False where the address
+// or a stride breaks the 16-byte rules of tensor copies; the kernel then
+// copies with cp.async.
+bool stream_map(CUtensorMap* m, const Launch& ln, const AxisParams& ap) {
+  const uint64_t C = sizeof(cpx);
+  const uint64_t s1 = uint64_t(ap.in_n) * C, s2 = uint64_t(ap.is1) * C, s3 = uint64_t(ap.is2) * C;
+  const uint64_t d2 = uint64_t(ln.st_d2);
+  if ((reinterpret_cast<uintptr_t>(ap.in) & 15) || (s1 & 15) || (ap.d1 > 1 && (s2 & 15)) || (d2 > 1 && (s3 & 15)))
+    return false;
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const cuuint64_t dims[4] = {cuuint64_t(2 * ap.d0), cuuint64_t(ln.L), cuuint64_t(ap.d1), cuuint64_t(d2)};
+  // unit extents get a harmless stride (the coordinate is always 0)
+  const uint64_t span1 = s1 * uint64_t(ln.L);
+  const uint64_t st1 = ap.d1 > 1 ? s2 : (span1 + 15) / 16 * 16;
+  const uint64_t st2 = d2 > 1 ? s3 : (st1 * uint64_t(ap.d1) + 15) / 16 * 16;
+  const cuuint64_t strides[3] = {cuuint64_t(s1), cuuint64_t(st1), cuuint64_t(st2)};
+  const cuuint32_t box[4] = {cuuint32_t(2 * mb::stream_cols()), cuuint32_t(ln.L < 256 ? ln.L : 256), 1, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  for (int i = 0; i < 3; ++i)
+    if (strides[i] >= (uint64_t(1) << 40)) return false;
+  const CUtensorMapDataType dt = sizeof(real) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(m, dt, 4, const_cast<void*>(ap.in), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor map of a streamed tensor-core pass's input (complex single
+// precision): column tiles dims (2*d0 reals, 256 points, d1, d2), box (32
+// reals, 128 points); row tiles dims (512 reals, d0 transforms, d1, d2), box
+// (256 reals, 16 transforms).
+bool tc_stream_map(CUtensorMap* m, const Launch& ln, const AxisParams& ap) {
+  const uint64_t C = sizeof(cpx);
+  const uint64_t d2 = uint64_t(ln.st_d2);
+  const bool rows = ln.tcs == 2;
+  const uint64_t s1 = rows ? uint64_t(ap.is0) * C : uint64_t(ap.in_n) * C;
+  const uint64_t s2 = uint64_t(ap.is1) * C, s3 = uint64_t(ap.is2) * C;
+  if ((reinterpret_cast<uintptr_t>(ap.in) & 15) || (s1 & 15) || (ap.d1 > 1 && (s2 & 15)) || (d2 > 1 && (s3 & 15)))
+    return false;
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const uint64_t n1 = rows ? uint64_t(ap.d0) : uint64_t(ln.L);
+  const cuuint64_t dims[4] = {cuuint64_t(rows ? 2 * ln.L : 2 * ap.d0), cuuint64_t(n1), cuuint64_t(ap.d1),
+                              cuuint64_t(d2)};
+  const uint64_t st1 = ap.d1 > 1 ? s2 : (s1 * n1 + 15) / 16 * 16;
+  const uint64_t st2 = d2 > 1 ? s3 : (st1 * uint64_t(ap.d1) + 15) / 16 * 16;
+  const cuuint64_t strides[3] = {cuuint64_t(s1), cuuint64_t(st1), cuuint64_t(st2)};
+  for (int i = 0; i < 3; ++i)
+    if (strides[i] >= (uint64_t(1) << 40)) return false;
+  const cuuint32_t box[4] = {cuuint32_t(rows ? 256 : 32), cuuint32_t(rows ? 16 : 128), 1, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(ap.in), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
   void* args[1];
   if (ln.is_line) {
@@ -1420,12 +1704,31 @@ bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
     while (ch > 4 && (reinterpret_cast<uintptr_t>(ap.in) % ch) != 0) ch /= 2;
     ap.chunk = ch;
   }
+  if (ln.stream) {
+    alignas(64) CUtensorMap map;
+    memset(&map, 0, sizeof(map));
+    if (stream_map(&map, ln, ap))
+      ap.flags |= mb::F_STREAM_TMA;
+    else if (reinterpret_cast<uintptr_t>(ap.in) % sizeof(cpx)) {
+      set_error(MINFFT_B200_EINVAL, "complex input not aligned to its size");
+      return false;
+    }
+    void* sargs[2] = {&ap, &map};
+    return enqueue(a, ln, sargs, ln.smem, "launch(stream)");
+  }
   if (ln.tc) {
     mb::TcParams tcp = ln.tcp;
     const long long withhold = g_tc_withhold.load();
     if (withhold > 0) {
       tcp.withhold = 1;
       tcp.wait_polls = withhold;
+    }
+    if (ln.tcs) {
+      alignas(64) CUtensorMap map;
+      memset(&map, 0, sizeof(map));
+      if (tc_stream_map(&map, ln, ap)) ap.flags |= mb::F_STREAM_TMA;
+      void* sargs[3] = {&ap, &tcp, &map};
+      return enqueue(a, ln, sargs, ln.smem, "launch(tc stream)");
     }
     void* targs[2] = {&ap, &tcp};
     return enqueue(a, ln, targs, ln.smem, "launch(tc)");
@@ -1951,15 +2254,30 @@ MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns,
            (long long)((e.out_max + 1) * oe), ln.out_buf, cap[ln.out_buf]);
     if (ln.block < 1 || ln.block > 1024 || ln.grid < 1) fail("launch %zu: bad shape %u x %u", i, ln.grid, ln.block);
     if (!ln.is_line && ln.block > 512) fail("launch %zu: block %u above launch bounds", i, ln.block);
-    if (!ln.is_line && ln.block != unsigned(ln.ap.cpb * (ln.L / std::min(ln.radix, std::max(ln.L, 1)))))
+    if (!ln.is_line && !ln.stream && !ln.tcs &&
+        ln.block != unsigned(ln.ap.cpb * (ln.L / std::min(ln.radix, std::max(ln.L, 1)))))
       fail("launch %zu: block %u is not cpb x L/R", i, ln.block);
     if (ln.smem > size_t(di.max_smem)) fail("launch %zu: %zu bytes of shared memory", i, ln.smem);
     const bool alias_io = (ln.in_buf == ln.out_buf) || (alias && ((ln.in_buf == BUF_X && ln.out_buf == BUF_Y) ||
                                                                  (ln.in_buf == BUF_Y && ln.out_buf == BUF_X)));
     if (alias_io && (ln.hbm_pass || (ln.is_line && ln.combo != mb::LK_UNIT)))
       fail("launch %zu (%s): runs in place but cannot", i, ln.label.c_str());
-    if (!ln.is_line && !ln.pipe && !ln.tc && ln.grid > 0 && int64_t(ln.grid) * ln.ap.cpb < ln.ap.nbatch)
+    if (!ln.is_line && !ln.pipe && !ln.tc && !ln.stream && ln.grid > 0 &&
+        int64_t(ln.grid) * ln.ap.cpb < ln.ap.nbatch)
       fail("launch %zu: grid does not cover the batch", i);
+    if (ln.stream) {
+      const AxisParams& ap = ln.ap;
+      const int W = mb::stream_cols();
+      if (ap.is0 != 1 || !ap.colmode || ln.combo != mb::K_CPLX)
+        fail("launch %zu (%s): streamed pass needs adjacent unit-stride columns", i, ln.label.c_str());
+      if (ap.d0 * ap.d1 * ln.st_d2 != ap.nbatch || ap.gpb * W < ap.d0 || ap.ntiles != ap.gpb * ap.d1 * ln.st_d2)
+        fail("launch %zu (%s): streamed tiles do not cover the batch", i, ln.label.c_str());
+      if (ln.block != unsigned(W * (ln.L / ln.radix)) || ap.cpb < 2 || ap.cpb > 8)
+        fail("launch %zu: streamed shape %u threads, %d stages", i, ln.block, ap.cpb);
+      if (size_t(ap.stage_bytes) < size_t(W) * (ln.L + 1) * sizeof(cpx) || ap.stage_bytes % 128)
+        fail("launch %zu: stage of %d bytes", i, ap.stage_bytes);
+      if (ln.grid < 1 || int64_t(ln.grid) > ap.ntiles) fail("launch %zu: persistent grid %u", i, ln.grid);
+    }
     if (ln.pipe) {
       const AxisParams& ap = ln.ap;
       if (ap.colmode) {
@@ -1985,9 +2303,21 @@ MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns,
     if (ln.tc) {
       if (ln.L != mb::kTcLength || ln.combo != mb::K_CPLX)
         fail("launch %zu (%s): tensor-core pass on an unsupported axis", i, ln.label.c_str());
-      if (ln.ap.cpb != 8 && ln.ap.cpb != 16) fail("launch %zu: tensor-core tile of %d transforms", i, ln.ap.cpb);
-      if (ln.ap.ntiles * ln.ap.cpb < ln.ap.nbatch || ln.grid < 1 || int64_t(ln.grid) > ln.ap.ntiles)
-        fail("launch %zu: tensor-core tiles do not cover the batch", i);
+      if (ln.tcs) {
+        const AxisParams& ap = ln.ap;
+        const int W = mb::kTcStreamTile;
+        if ((ln.tcs == 1) != (ap.colmode != 0) || (ap.colmode ? ap.is0 != 1 : ap.in_n != 1))
+          fail("launch %zu (%s): streamed tensor-core tile layout", i, ln.label.c_str());
+        if (ap.d0 * ap.d1 * ln.st_d2 != ap.nbatch || ap.gpb * W < ap.d0 || ap.ntiles != ap.gpb * ap.d1 * ln.st_d2)
+          fail("launch %zu (%s): streamed tensor-core tiles do not cover the batch", i, ln.label.c_str());
+        if (ln.block != unsigned(mb::kTcStreamThreads) || ap.cpb < 2 || ap.cpb > 8 || ln.grid < 1 ||
+            int64_t(ln.grid) > ap.ntiles)
+          fail("launch %zu: streamed tensor-core shape", i);
+      } else {
+        if (ln.ap.cpb != 8 && ln.ap.cpb != 16) fail("launch %zu: tensor-core tile of %d transforms", i, ln.ap.cpb);
+        if (ln.ap.ntiles * ln.ap.cpb < ln.ap.nbatch || ln.grid < 1 || int64_t(ln.grid) > ln.ap.ntiles)
+          fail("launch %zu: tensor-core tiles do not cover the batch", i);
+      }
     }
   }
   if (launches) *launches = (int)prog.launches.size();
@@ -2066,14 +2396,23 @@ MB_EXPORT int minfft_b200_autotune(minfft_aux* a, int op, int howmany, int reps)
     Planner probe{a, nullptr, di.max_smem, di.sms};
     float best_ms = 1e30f;
     TuneVal best_v{0, 0, 16};
-    for (int cand = 0; cand < 4; ++cand) {
-      const int pipe = cand & 1, radix = (cand & 2) ? 8 : 16;
+    // the launch's own parameters (for the streamed form's applicability)
+    const Launch* base = nullptr;
+    for (const Launch& ln : p0->launches)
+      if (!ln.is_line && !ln.tc && !(ln.key < key) && !(key < ln.key)) base = &ln;
+    for (int cand = 0; cand < 6; ++cand) {
+      const int pipe = cand < 4 ? (cand & 1) : 2, radix = (cand & 2) ? 8 : 16;
       if (radix == 8 && key.L <= 8) continue;
-      for (int cpb = 1; cpb <= probe.max_threads_cpb(key.L, radix); cpb *= 2) {
+      const int top = pipe == 2 ? 4 : probe.max_threads_cpb(key.L, radix);
+      for (int cpb = pipe == 2 ? 2 : 1; cpb <= top; cpb = pipe == 2 ? cpb + 1 : 2 * cpb) {
         if (Planner::four_rows(key.combo) && (pipe || cpb != 4)) continue;
-        const bool fits = pipe ? probe.pipe_fits(key.combo, key.L, cpb, key.colmode, radix)
-                               : probe.plain_fits(key.combo, key.L, cpb, key.staged ? mb::F_STAGE_ROWS : 0,
-                                                  key.colmode, radix);
+        bool fits;
+        if (pipe == 2)
+          fits = base && probe.stream_fits(key.combo, key.L, base->ap.nbatch, base->ap, radix, cpb);
+        else if (pipe == 1)
+          fits = probe.pipe_fits(key.combo, key.L, cpb, key.colmode, radix);
+        else
+          fits = probe.plain_fits(key.combo, key.L, cpb, key.staged ? mb::F_STAGE_ROWS : 0, key.colmode, radix);
         if (!fits) continue;
         force[key] = TuneVal{pipe, cpb, radix};
         Program P;
@@ -2149,7 +2488,7 @@ MB_EXPORT int minfft_b200_tune_load(const char* path) {
     long long nb, d0, in_n, out_k;
     if (sscanf(line, "%d %d %d %d %d %lld %lld %lld %lld %d %d %d", &k.combo, &k.L, &k.colmode, &k.hbm, &k.staged,
                &nb, &d0, &in_n, &out_k, &v.pipe, &v.cpb, &v.radix) == 12 &&
-        (v.radix == 8 || v.radix == 16)) {
+        (v.radix == 8 || v.radix == 16) && v.pipe >= 0 && v.pipe <= 2) {
       k.nbatch = nb;
       k.d0 = d0;
       k.in_n = in_n;
@@ -2179,7 +2518,7 @@ MB_EXPORT int minfft_b200_tune_size(void) {
 // built afterwards use it.
 MB_EXPORT int minfft_b200_tune_set_default(int pipe, int cpb, int radix) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_default_override = TuneVal{pipe < 0 ? -1 : (pipe ? 1 : 0), cpb < 0 ? 0 : cpb, radix == 8 ? 8 : 16};
+  g_default_override = TuneVal{pipe < 0 ? -1 : (pipe >= 2 ? 2 : (pipe ? 1 : 0)), cpb < 0 ? 0 : cpb, radix == 8 ? 8 : 16};
   return MINFFT_B200_OK;
 }
 

@@ -49,6 +49,7 @@
 #include <cmath>
 
 #include "axis_pass.cuh"
+#include "stream_pass.cuh"
 #include "tc_pass.h"
 
 namespace mb {
@@ -525,6 +526,403 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
   }
 }
 
+
+// ===================================================== streamed TC pass
+// The same two radix-16 contractions, on the tile pipeline of the streamed
+// column pass (stream_pass.cuh): persistent CTAs, tiles of 16 transforms of
+// 256 points copied into S shared-memory stages by tensor copies (or
+// cp.async where the strides do not allow them), an mbarrier per stage.
+//
+// Thread t owns row t of the contraction: in stage 1 the sub-DFT (c, n2) --
+// inputs x[16 n1 + n2], n1 = 0..15 -- and in stage 2 the sub-DFT (c, k1) --
+// inputs y1[16 k1 + n2] after the twiddles, n2 = 0..15 -- with c the
+// transform of the tile and the digit d = n2 (stage 1) or k1 (stage 2):
+// column tiles c = t % 16, d = t / 16; row tiles d = t % 16, c = t / 16, so
+// that in both the 16 threads of a half warp read 128 contiguous bytes of
+// the tile.  Each row is scaled by its own power of two (largest component
+// into [2^8, 2^9)), split into NT 16-bit terms and written as row t of the
+// K-major A operand of its group of 128 rows; thread 0 issues the MMAs of
+// both groups (corrections into one accumulator, the leading product into
+// another) and commits them to an mbarrier; every thread reads its row of
+// both accumulators with one tcgen05.ld each, adds them and unscales.
+//
+// Between the stages the twiddled values go back into the stage, which then
+// holds y1 in a layout chosen per tile kind so that the writes (lanes over
+// n2) and the reads (lanes over k1) are both conflict-free: column tiles
+// (16 k1 + n2) * 16 + c, row tiles c * 256 + 16 k1 + (n2 ^ k1).
+constexpr int kTcsW = 16;     // transforms per tile
+constexpr int kTcsNT = 256;   // threads
+constexpr int kTcsStages = 2;
+
+template <int FMT>
+struct TcsLayout {
+  static constexpr int NT = FMT == TC_F16 ? 2 : 3;
+  static constexpr int bar_bytes = 128;                  // mbarriers, TMEM slot, flag
+  static constexpr int b_off = bar_bytes;                // B operands: NT x 2 KB
+  static constexpr int a_off = b_off + NT * kBBytes;     // A operands: 2 groups x NT x 8 KB
+  static constexpr int st_off = a_off + 2 * NT * kOpBytes;
+  static constexpr int tmem_cols = 128;                  // 2 groups x (leading, correction) x 32
+};
+
+__host__ __device__ inline int tcs_stage_bytes() { return (kTcsW * (kL + 1) * 8 + 127) / 128 * 128; }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&d)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), "=r"(d[8]),
+        "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]), "=r"(d[16]),
+        "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]), "=r"(d[24]),
+        "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
+      : "r"(taddr)
+      : "memory");
+}
+
+// Power-of-two scale putting the largest component of 16 complex values
+// into [2^8, 2^9): returns the scale; *inv receives its inverse.
+__device__ __forceinline__ float tcs_scale(const float (&re)[16], const float (&im)[16], float* inv) {
+  float mx = 0.f;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) mx = fmaxf(mx, fmaxf(fabsf(re[i]), fabsf(im[i])));
+  const int ex = (__float_as_int(mx) >> 23) & 0xFF;
+  const int s = min(max(135 - ex, -126), 126);
+  *inv = pow2i(-s);
+  return pow2i(s);
+}
+
+// Split row (re, im) * sc into NT terms and write them as row `row` of the
+// K-major A operands of group g (K: Re 0..15, Im 16..31).
+template <int FMT>
+__device__ __forceinline__ void tcs_write_a(unsigned char* aop, int g, int row, const float (&re)[16],
+                                            const float (&im)[16], float sc) {
+  constexpr int NT = TcsLayout<FMT>::NT;
+#pragma unroll
+  for (int kb = 0; kb < 4; ++kb) {
+    uint32_t w[NT][4];
+#pragma unroll
+    for (int u = 0; u < 8; u += 2) {
+      uint32_t o[3];
+      const int k = kb * 8 + u;
+      const float a = k < 16 ? re[k] : im[k - 16], b = k + 1 < 16 ? re[k + 1] : im[k + 1 - 16];
+      split_pair<FMT, NT>(a * sc, b * sc, o);
+#pragma unroll
+      for (int z = 0; z < NT; ++z) w[z][u / 2] = o[z];
+    }
+#pragma unroll
+    for (int z = 0; z < NT; ++z)
+      *reinterpret_cast<uint4*>(aop + (z * 2 + g) * kOpBytes + tc_operand_offset(row, kb * 8)) =
+          make_uint4(w[z][0], w[z][1], w[z][2], w[z][3]);
+  }
+}
+
+// Thread 0: the MMAs of both groups for the A operands in place, committed
+// to mbarrier `mb`.
+template <int FMT>
+__device__ __forceinline__ void tcs_issue_mma(uint32_t aop_a, uint32_t bop_a, uint32_t tmem, uint32_t mb) {
+  constexpr int NT = TcsLayout<FMT>::NT;
+  constexpr uint32_t idesc = instr_desc<FMT>();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int sum = NT - 1; sum >= 1; --sum)
+#pragma unroll
+      for (int i = 0; i <= sum; ++i) {
+        const int j = sum - i;
+#pragma unroll
+        for (int kh = 0; kh < 2; ++kh) {
+          const uint64_t ad = smem_desc(aop_a + (i * 2 + g) * kOpBytes + kh * 256);
+          const uint64_t bd = smem_desc(bop_a + j * kBBytes + kh * 256);
+          mma_f16(tmem + uint32_t(64 * g + 32), ad, bd, idesc, acc);
+          acc = 1;
+        }
+      }
+#pragma unroll
+    for (int kh = 0; kh < 2; ++kh) {
+      const uint64_t ad = smem_desc(aop_a + g * kOpBytes + kh * 256);
+      const uint64_t bd = smem_desc(bop_a + kh * 256);
+      mma_f16(tmem + uint32_t(64 * g), ad, bd, idesc, kh);
+    }
+  }
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb) : "memory");
+}
+
+// This thread's row of both accumulators, summed: re[k], im[k], k = 0..15.
+__device__ __forceinline__ void tcs_read_d(uint32_t tmem, int warp, float (&re)[16], float (&im)[16]) {
+  const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(64 * (warp >> 2));
+  uint32_t d[32], e[32];
+  tmem_ld32(taddr, d);
+  tmem_ld32(taddr + 32, e);
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    re[k] = __uint_as_float(d[k]) + __uint_as_float(e[k]);
+    im[k] = __uint_as_float(d[16 + k]) + __uint_as_float(e[16 + k]);
+  }
+}
+
+template <int FMT, bool ROWS>
+__global__ void __launch_bounds__(kTcsNT, 1) tc_stream_kernel(const AxisParams p, const TcParams q,
+                                                              const __grid_constant__ CUtensorMap tmap) {
+  using Lay = TcsLayout<FMT>;
+  constexpr int NT = Lay::NT;
+  constexpr int W = kTcsW;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm);  // [0, 8): stage barriers, [8]: MMA barrier
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + 80);
+  int* bad = reinterpret_cast<int*>(sm + 84);
+  unsigned char* bop = sm + Lay::b_off;
+  unsigned char* aop = sm + Lay::a_off;
+  unsigned char* stages = sm + Lay::st_off;
+  const int S = p.cpb;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int c = ROWS ? tid / 16 : tid % 16;  // transform of the tile
+  const int d = ROWS ? tid % 16 : tid / 16;  // digit: n2 in stage 1, k1 in stage 2
+  const int g = tid >> 7, row = tid & 127;   // UMMA group and row
+  const bool tma = (p.flags & F_STREAM_TMA) != 0;
+  const uint32_t bar0 = static_cast<uint32_t>(__cvta_generic_to_shared(bars));
+  const uint32_t mma_bar = bar0 + 64;
+  const uint32_t st0 = static_cast<uint32_t>(__cvta_generic_to_shared(stages));
+  const uint32_t aop_a = static_cast<uint32_t>(__cvta_generic_to_shared(aop));
+  const uint32_t bop_a = static_cast<uint32_t>(__cvta_generic_to_shared(bop));
+  const int sb = p.stage_bytes;
+  const int64_t gpd = (p.d0 + W - 1) / W;
+  const int64_t ntiles = p.ntiles;
+
+  pdl_release();
+  pdl_wait();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(tslot))),
+                 "n"(Lay::tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) smbar_init(bar0 + 8 * s, tma ? 1 : kTcsNT);
+    smbar_init(mma_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *bad = 0;
+  }
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(q.bmat);
+    uint4* dst = reinterpret_cast<uint4*>(bop);
+    for (int i = tid; i < NT * kBBytes / 16; i += kTcsNT) dst[i] = src[i];
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  auto tile_pos = [&](int64_t t, int64_t& c0, int64_t& b1, int64_t& b2) {
+    const int64_t rest = t / gpd;
+    c0 = (t - rest * gpd) * W;
+    b1 = rest % p.d1;
+    b2 = rest / p.d1;
+  };
+  // tile element (transform cc, point n) -> complex index in the stage
+  auto pos_in = [&](int cc, int n) { return ROWS ? (n >> 7) * (W * 128) + cc * 128 + (n & 127) : n * W + cc; };
+
+  auto issue = [&](int64_t t, int s) {
+    if (t >= ntiles) return;
+    int64_t c0, b1, b2;
+    tile_pos(t, c0, b1, b2);
+    const uint32_t mb = bar0 + 8 * s;
+    const uint32_t dst = st0 + uint32_t(s) * uint32_t(sb);
+    if (tma) {
+      if (tid == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(W * kL * 8) : "memory");
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          // column tiles: box (32 reals = 16 transforms, 128 points); row
+          // tiles: box (256 reals = 128 points, 16 transforms)
+          const int x0 = ROWS ? 256 * h : int(2 * c0);
+          const int x1 = ROWS ? int(c0) : 128 * h;
+          asm volatile(
+              "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+              "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst + uint32_t(h * W * 128 * 8)),
+              "l"(&tmap), "r"(x0), "r"(x1), "r"(int(b1)), "r"(int(b2)), "r"(mb)
+              : "memory");
+        }
+      }
+    } else {
+      const int nv = int(p.d0 - c0 < W ? p.d0 - c0 : W);
+      const char* src = static_cast<const char*>(p.in) + (b1 * p.is1 + b2 * p.is2 + c0 * p.is0) * 8;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int e = tid + i * kTcsNT;
+        const int cc = ROWS ? e / kL : e % W, n = ROWS ? e % kL : e / W;
+        if (cc < nv) {
+          const char* gp = src + (int64_t(n) * p.in_n + cc * p.is0) * 8;
+          const uint32_t dd = dst + uint32_t(pos_in(cc, n) * 8);
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dd), "l"(gp) : "memory");
+        }
+      }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(mb) : "memory");
+    }
+  };
+
+  for (int s = 0; s < S; ++s) issue(blockIdx.x + int64_t(s) * gridDim.x, s);
+
+  const bool cj_in = (p.flags & F_CONJ_IN) != 0, cj_out = (p.flags & F_CONJ_OUT) != 0;
+  const bool rows_out = (p.flags & F_STAGE_ROWS) != 0;
+  const bool twid = p.st_ns > 1;
+  const long long first_limit = q.wait_polls > 0 ? q.wait_polls : kSpinLimit;
+  bool ok = true, pending = false, first = true;
+  uint32_t mph = 0;
+  int it = 0;
+  int64_t t = blockIdx.x;
+  for (; t < ntiles; t += gridDim.x, ++it) {
+    const int s = it % S;
+    if (!smbar_wait(bar0 + 8 * s, uint32_t(it / S) & 1u, kStreamSpinLimit)) atomicExch(bad, 1);
+    __syncthreads();
+    if (*bad) {
+      ok = false;
+      break;
+    }
+    cpx* tile = reinterpret_cast<cpx*>(stages + size_t(s) * sb);
+    int64_t c0, b1, b2;
+    tile_pos(t, c0, b1, b2);
+    const int64_t col = c0 + c;  // this thread's transform (b0 index)
+    const bool active = col < p.d0;
+    float re[16], im[16], inv;
+
+    // ---- stage 1: row (c, n2 = d), inputs x[16 n1 + d]
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+      const cpx u = tile[pos_in(c, 16 * n1 + d)];
+      re[n1] = u.x;
+      im[n1] = cj_in ? -u.y : u.y;
+    }
+    if (twid) {
+      // pre-twiddle of a later pass of a Stockham chain: element n = 16 n1 + d
+      // times w_Lt^(n * gq) = w^(d*gq) * (w^(16*gq))^n1
+      const int64_t gq = ((col / p.st_div) & (p.st_ns - 1)) << p.st_shift;
+      const cpx base = stockham_root(p, int64_t(d) * gq);
+      const cpx d1 = stockham_root(p, 16 * gq);
+      const cpx d2 = cmul(d1, d1);
+      const cpx d3 = cmul(d2, d1);
+      const cpx d4 = stockham_root(p, 64 * gq);
+      const cpx d8 = cmul(d4, d4);
+      const cpx d12 = cmul(d8, d4);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        cpx w = base;
+        if ((i >> 2) == 1) w = cmul(w, d4);
+        if ((i >> 2) == 2) w = cmul(w, d8);
+        if ((i >> 2) == 3) w = cmul(w, d12);
+        if ((i & 3) == 1) w = cmul(w, d1);
+        if ((i & 3) == 2) w = cmul(w, d2);
+        if ((i & 3) == 3) w = cmul(w, d3);
+        const cpx x = cmul(cmk(re[i], im[i]), w);
+        re[i] = x.x;
+        im[i] = x.y;
+      }
+    }
+    float sc = tcs_scale(re, im, &inv);
+    tcs_write_a<FMT>(aop, g, row, re, im, sc);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    const bool withheld = first && q.withhold;
+    if (tid == 0 && !withheld) tcs_issue_mma<FMT>(aop_a, bop_a, tmem, mma_bar);
+    pending = !withheld;
+    if (!smbar_wait(mma_bar, mph, first ? first_limit : kSpinLimit)) atomicExch(bad, 1);
+    first = false;
+    __syncthreads();
+    if (*bad) {
+      ok = false;
+      break;
+    }
+    pending = false;
+    mph ^= 1;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    tcs_read_d(tmem, warp, re, im);
+    // unscale and twiddle: y1[k1][n2] * w_256^(n2 k1), n2 = d; into the stage
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) {
+      const cpx w = ldg(p.tw + d * k1);
+      const cpx y = cmul(cmk(re[k1] * inv, im[k1] * inv), w);
+      const int idx = ROWS ? c * kL + 16 * k1 + (d ^ k1) : (16 * k1 + d) * W + c;
+      tile[idx] = y;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+
+    // ---- stage 2: row (c, k1 = d), inputs y1[16 d + n2], n2 = 0..15
+#pragma unroll
+    for (int n2 = 0; n2 < 16; ++n2) {
+      const int idx = ROWS ? c * kL + 16 * d + (n2 ^ d) : (16 * d + n2) * W + c;
+      const cpx u = tile[idx];
+      re[n2] = u.x;
+      im[n2] = u.y;
+    }
+    sc = tcs_scale(re, im, &inv);
+    tcs_write_a<FMT>(aop, g, row, re, im, sc);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) tcs_issue_mma<FMT>(aop_a, bop_a, tmem, mma_bar);
+    pending = true;
+    if (!smbar_wait(mma_bar, mph, kSpinLimit)) atomicExch(bad, 1);
+    __syncthreads();
+    if (*bad) {
+      ok = false;
+      break;
+    }
+    pending = false;
+    mph ^= 1;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    tcs_read_d(tmem, warp, re, im);
+    const float so = cj_out ? -inv : inv;
+    // outputs y[k1 + 16 k2], k1 = d
+    cpx* out = static_cast<cpx*>(p.out);
+    const int64_t ob = b1 * p.os1 + b2 * p.os2;
+    if (!rows_out) {
+      if (active) {
+        cpx* o = out + ob + col * p.os0 + int64_t(d) * p.out_k;
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) o[int64_t(16 * k2) * p.out_k] = cmk(re[k2] * inv, im[k2] * so);
+      }
+    } else {
+      // contiguous outputs per transform: transpose through the stage
+      // (transform c at c*(256+1)), then store with k running fastest
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) tile[c * (kL + 1) + d + 16 * k2] = cmk(re[k2] * inv, im[k2] * so);
+      __syncthreads();
+      const int nv = int(p.d0 - c0 < W ? p.d0 - c0 : W);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int e = tid + i * kTcsNT;
+        const int cc = e / kL, k = e % kL;
+        if (cc < nv) out[ob + (c0 + cc) * p.os0 + int64_t(k) * p.out_k] = tile[cc * (kL + 1) + k];
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();  // the stage and the accumulators are free
+    if (tma && tid == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    issue(t + int64_t(S) * gridDim.x, s);
+  }
+
+  if (!ok) {
+    if (tid == 0 && q.status) atomicExch(q.status, 1);
+    if (pending) mbar_wait(mma_bar, mph);
+    for (int k = 0; k < S; ++k, ++it, t += gridDim.x) {
+      if (t >= ntiles) break;
+      smbar_wait(bar0 + 8 * (it % S), uint32_t(it / S) & 1u, kStreamSpinLimit);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(Lay::tmem_cols)
+                 : "memory");
+  }
+}
+
 }  // namespace
 
 const void* tc_kernel(int fmt, int tb) {
@@ -543,10 +941,27 @@ size_t tc_smem(int fmt, int tb) {
   return tb == 8 ? TcLayout<TC_BF16, 8>::total : TcLayout<TC_BF16, 16>::total;
 }
 
+const void* tc_stream_kernel_fn(int fmt, bool rows) {
+  if (fmt == TC_F16) return rows ? (const void*)tc_stream_kernel<TC_F16, true> : (const void*)tc_stream_kernel<TC_F16, false>;
+  if (fmt == TC_BF16)
+    return rows ? (const void*)tc_stream_kernel<TC_BF16, true> : (const void*)tc_stream_kernel<TC_BF16, false>;
+  return nullptr;
+}
+
+size_t tc_stream_smem(int fmt, int stages) {
+  const size_t st = fmt == TC_F16 ? TcsLayout<TC_F16>::st_off : TcsLayout<TC_BF16>::st_off;
+  return st + size_t(stages) * tcs_stage_bytes();
+}
+
+int tc_stream_stage_bytes() { return tcs_stage_bytes(); }
+
 #else
 
 const void* tc_kernel(int, int) { return nullptr; }
 size_t tc_smem(int, int) { return 0; }
+const void* tc_stream_kernel_fn(int, bool) { return nullptr; }
+size_t tc_stream_smem(int, int) { return 0; }
+int tc_stream_stage_bytes() { return 0; }
 
 #endif
 

@@ -89,7 +89,7 @@ def test_tc_in_place(mode):
 @pytest.mark.parametrize("mode", MODES)
 def test_tc_uses_tensor_core_kernels(mode):
     names = labels((64, 256), mode)
-    assert any(n.startswith("tc_pass<") for n in names), names
+    assert any(n.startswith(("tc_pass<", "tc_stream<")) for n in names), names
     assert not any(n.startswith("axis_pass<cplx,L=256") for n in names), names
     # back to FP32: no tensor-core launch
     eng = minfft_b200.engine(True)
@@ -100,7 +100,7 @@ def test_tc_uses_tensor_core_kernels(mode):
         x = torch.zeros((64, 256), dtype=torch.complex64, device="cuda")
         eng.profile(plan.aux, 1)
         plan("dft", x.data_ptr(), x.data_ptr())
-        assert not any(s[0].startswith("tc_pass<") for s in eng.profile_stats(plan.aux))
+        assert not any(s[0].startswith(("tc_pass<", "tc_stream<")) for s in eng.profile_stats(plan.aux))
     finally:
         plan.free()
 
@@ -110,7 +110,7 @@ def test_tc_passes_of_long_column_axis(mode):
     """65536-point columns: two HBM passes of 256, both on tensor cores."""
     dims = (65536, 2)
     names = labels(dims, mode)
-    assert any(n.startswith("tc_pass<") for n in names), names
+    assert any(n.startswith(("tc_pass<", "tc_stream<")) for n in names), names
     x = data(dims, 3)
     got = run("dft", x, dims, mode)
     err = rel_l2(got, ref("dft", x, dims))
@@ -132,7 +132,7 @@ def tc_launches(dims, mode, op="dft"):
         y = torch.empty_like(x)
         eng.profile(plan.aux, 1)
         plan(op, x.data_ptr(), y.data_ptr())
-        return sum(s[1] for s in eng.profile_stats(plan.aux) if s[0].startswith("tc_pass<"))
+        return sum(s[1] for s in eng.profile_stats(plan.aux) if s[0].startswith(("tc_pass<", "tc_stream<")))
     finally:
         plan.free()
 

@@ -142,9 +142,9 @@ TC_CHAINS = [(1 << 16, ["tc:256", "tc:256"]), (1 << 20, ["tc:256", "cplx:4096"])
 def chain_passes(report):
     out = []
     for lab in report.splitlines():
-        m = re.search(r"(tc_pass|axis_pass|axis_pipe)<([a-z0-9+]+)?[^,]*,L=(\d+)", lab)
+        m = re.search(r"(tc_pass|tc_stream|axis_pass|axis_pipe|stream_pass)<([a-z0-9+]+)?[^,]*,L=(\d+)", lab)
         if m:
-            out.append(("tc" if m.group(1) == "tc_pass" else m.group(2)) + ":" + m.group(3))
+            out.append(("tc" if m.group(1) in ("tc_pass", "tc_stream") else m.group(2)) + ":" + m.group(3))
     return out
 
 
