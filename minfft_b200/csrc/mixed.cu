@@ -13,13 +13,19 @@
 // Execution (device).  Every resident CTA takes the next item from an
 // atomic counter until the list is exhausted.  Short items run the same
 // load -> Stockham passes -> store code as the axis passes, with each
-// transform's own input and output pointers.  A long item is handled by its
-// CTA alone: the kind's element-wise pre-processing, two Stockham passes over
-// global memory through the CTA's private scratch slice (rounds of 32 or 64
-// sub-DFTs of 128/256 points), and the post-processing.
+// transform's own input and output pointers.  Long items (2^14 .. 2^16
+// complex points) run on clusters of eight CTAs entirely in distributed
+// shared memory (mixed_cluster_kernel, run_cluster_big): the clusters take
+// the long items first, one per cluster, then every CTA takes short items on
+// its own.  Where the cluster form cannot be launched, the plain kernel runs
+// each long item on one CTA instead: the element-wise pre-processing, two
+// Stockham passes over global memory through the CTA's private scratch slice
+// and the post-processing.
 //
-// No CTA ever waits on another (the queue is a single atomicAdd per item),
-// so the kernel cannot deadlock whatever the residency.
+// No CTA ever waits on a CTA outside its own cluster (the queues are a
+// single atomicAdd per item; the CTAs of a cluster are co-resident by
+// construction), so the kernel cannot deadlock whatever the residency.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 
@@ -80,8 +86,8 @@ struct Params {
   const int* order;
   const Item* items;
   int nitems;
-  int pad;
-  unsigned* counter;
+  int nbig;            // items [0, nbig) are long items (cluster form), the rest short ones
+  unsigned* counter;   // [0]: next short item, [1]: next long item (cluster form)
   cpx* scratch;
   int64_t scratch_stride;  // complex elements per CTA (two buffers)
   const cpx* tw[kSlots];    // w_L^m, by log2 L
@@ -372,6 +378,294 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<16>::value) mixed_kernel(c
   }
 }
 
+// ------------------------------------------------- long items on a cluster
+// A long item (L = 2^14 .. 2^16 complex points) is computed by a cluster of
+// kCluster CTAs entirely in their shared memory (the four-step split
+// n = 256*n1 + n2, k = k1 + N1*k2, N1 = L/256): CTA r holds the 32 columns
+// n2 = 32r .. 32r+31 of all N1 rows, computes their length-N1 DFTs over n1
+// (with the kind's pre-processing fused into the global loads) and the
+// twiddles w_L^(n2 k1); after a cluster barrier it gathers, through
+// distributed shared memory, rows k1 = r*N1/8 .. (r+1)*N1/8-1 from all eight
+// CTAs and computes their length-256 DFTs over n2, then applies the kind's
+// post-processing (reading the partner outputs z_{L-k} of the real DFT and
+// DCT-2 from the CTA that holds them) and stores.  Each element is read from
+// and written to global memory once.
+constexpr int kCluster = 8;
+constexpr int kN2 = 256;
+constexpr int kColsPerCta = kN2 / kCluster;  // 32
+
+// Element n (< L) of the complex sequence whose length-L DFT a long item of
+// kind it.combo needs: the pre-processing steps of line_ops.cuh, per element.
+__device__ __forceinline__ cpx big_pre(const Params& mp, const Item& it, const Job& job, int LG, int64_t n) {
+  const int64_t L = int64_t(1) << LG, N = 2 * L;
+  const int log2N = LG + 1;
+  const bool dst = (it.flags & F_DST) != 0;
+  switch (it.combo) {
+    case K_CPLX: {
+      cpx x = static_cast<const cpx*>(job.in)[n];
+      if (it.flags & F_CONJ_IN) x.y = -x.y;
+      return x;
+    }
+    case K_R2C:
+      return static_cast<const cpx*>(job.in)[n];  // the real row as pairs (aligned: checked at planning)
+    case K_DCT2: {
+      const real* in = static_cast<const real*>(job.in);
+      const real sg = dst ? real(-1) : real(1);
+      const int64_t i0 = 2 * n, i1 = 2 * n + 1;
+      const real a = i0 < L ? in[2 * i0] : sg * in[2 * N - 1 - 2 * i0];
+      const real b = i1 < L ? in[2 * i1] : sg * in[2 * N - 1 - 2 * i1];
+      return cmk(a, b);
+    }
+    case K_T4: {
+      const real* in = static_cast<const real*>(job.in);
+      const real a = in[2 * n], b = in[N - 1 - 2 * n];
+      const cpx w = ldg(mp.t4a[log2N] + n);
+      if (!dst) return cmul(w, cmk(a, b));
+      const cpx q = cmul(w, cmk(a, -b));
+      return cmk(-q.x, -q.y);
+    }
+    default: {  // K_C2R and K_DCT3: packing of the pair (n, L-n), conjugated
+      const cpx* zin = static_cast<const cpx*>(job.in);
+      const real* rin = static_cast<const real*>(job.in);
+      auto z = [&](int64_t k) -> cpx {
+        if (it.combo == K_C2R) return zin[k];
+        auto rd = [&](int i) { return rin[i]; };
+        return LoadDCT3::zval_r(rd, int(k), int(L), dst, mp.t23[log2N]);
+      };
+      const cpx* rft = mp.rft[log2N];
+      if (n == 0) {
+        const cpx z0 = z(0), z1 = z(L);
+        return cmk(z0.x + z1.x, -(z0.x - z1.x));
+      }
+      if (2 * n == L) {
+        const cpx z0 = z(n);
+        return cmk(2 * z0.x, 2 * z0.y);
+      }
+      cpx ta, tb;
+      if (2 * n < L) {
+        pack_pair(z(n), z(L - n), ldg(rft + n), ta, tb);
+        return cconj(ta);
+      }
+      pack_pair(z(L - n), z(n), ldg(rft + (L - n)), ta, tb);
+      return cconj(tb);
+    }
+  }
+}
+
+// Outputs of a long item for DFT output z_k of a kind without pairing.
+__device__ __forceinline__ void big_post_single(const Params& mp, const Item& it, const Job& job, int LG, int64_t k,
+                                                cpx zk) {
+  const int64_t L = int64_t(1) << LG, N = 2 * L;
+  const int log2N = LG + 1;
+  const bool dst = (it.flags & F_DST) != 0;
+  switch (it.combo) {
+    case K_CPLX:
+      if (it.flags & F_CONJ_OUT) zk.y = -zk.y;
+      static_cast<cpx*>(job.out)[k] = zk;
+      break;
+    case K_C2R:
+      static_cast<cpx*>(job.out)[k] = cconj(zk);  // the real output as pairs (aligned: checked at planning)
+      break;
+    case K_DCT3: {
+      real* out = static_cast<real*>(job.out);
+      const cpx w = cconj(zk);
+      const int64_t i0 = 2 * k, i1 = 2 * k + 1;
+      const real a = (dst && i0 >= L) ? -w.x : w.x;
+      const real b = (dst && i1 >= L) ? -w.y : w.y;
+      out[i0 < L ? 2 * i0 : 2 * N - 1 - 2 * i0] = a;
+      out[i1 < L ? 2 * i1 : 2 * N - 1 - 2 * i1] = b;
+      break;
+    }
+    default: {  // K_T4
+      real* out = static_cast<real*>(job.out);
+      const cpx* t4b = mp.t4b[log2N];
+      const cpx a = cmul(ldg(t4b + 2 * k), zk);
+      const cpx b = cmul(ldg(t4b + (N - 1 - 2 * k)), cconj(zk));
+      out[2 * k] = 2 * (dst ? a.y : a.x);
+      out[N - 1 - 2 * k] = 2 * (dst ? b.y : b.x);
+      break;
+    }
+  }
+}
+
+// Outputs of the pairing kinds (real DFT, DCT-2) from z_k and z_{L-k}, for
+// 0 <= k <= L/2 (k = 0 also covers X_L; zb is unused there and at k = L/2).
+__device__ __forceinline__ void big_post_pair(const Params& mp, const Item& it, const Job& job, int LG, int64_t k,
+                                              cpx za, cpx zb) {
+  const int64_t L = int64_t(1) << LG, N = 2 * L;
+  const int log2N = LG + 1;
+  const cpx* rft = mp.rft[log2N];
+  if (it.combo == K_R2C) {
+    cpx* out = static_cast<cpx*>(job.out);
+    if (k == 0) {
+      out[0] = cmk(za.x + za.y, real(0));
+      out[L] = cmk(za.x - za.y, real(0));
+    } else if (2 * k == L) {
+      out[k] = cconj(za);
+    } else {
+      cpx xa, xb;
+      unpack_pair(za, zb, ldg(rft + k), xa, xb);
+      out[k] = xa;
+      out[L - k] = xb;
+    }
+    return;
+  }
+  real* out = static_cast<real*>(job.out);
+  const bool dst = (it.flags & F_DST) != 0;
+  const cpx* t23 = mp.t23[log2N];
+  if (k == 0) {
+    const real r2 = real(1.414213562373095048801688724209698079);
+    out[dst ? N - 1 : 0] = 2 * (za.x + za.y);
+    out[dst ? L - 1 : L] = r2 * (za.x - za.y);
+  } else if (2 * k == L) {
+    StoreDCT2::emit(out, 1, int(k), int(N), dst, cconj(za), ldg(t23 + k));
+  } else {
+    cpx xa, xb;
+    unpack_pair(za, zb, ldg(rft + k), xa, xb);
+    StoreDCT2::emit(out, 1, int(k), int(N), dst, xa, ldg(t23 + k));
+    StoreDCT2::emit(out, 1, int(L - k), int(N), dst, xb, ldg(t23 + (L - k)));
+  }
+}
+
+template <int LG>
+__device__ __noinline__ void run_cluster_big(const Params& mp, const Item& it, unsigned char* smem) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  constexpr int L = 1 << LG;
+  constexpr int N1 = L / kN2;                 // 64, 128, 256
+  constexpr int TPT1 = kThreads / kColsPerCta;  // 16 threads per column in step 1
+  constexpr int R1 = N1 / TPT1;               // 4, 8, 16
+  constexpr int K1 = N1 / kCluster;           // rows k1 per CTA in step 2: 8, 16, 32
+  constexpr int TPT2 = kThreads / K1;         // 64, 32, 16
+  constexpr int R2 = kN2 / TPT2;              // 4, 8, 16
+  static_assert(R1 >= 4 && R2 >= 4 && TPT1 * kColsPerCta == kThreads, "shape");
+  const int rank = int(cl.block_rank());
+  const Job job = mp.jobs[mp.order[it.first]];
+  cpx* tile = reinterpret_cast<cpx*>(smem + kOffsetsBytes);
+  const int lp1 = tile_pitch(N1, R1, kColsPerCta, 1);
+  const int lp2 = tile_pitch(kN2, R2, K1, 1);
+  const int lobits = (LG + 1) / 2;
+  const int64_t lomask = (int64_t(1) << lobits) - 1;
+
+  // ---- step 1: DFTs over n1 of the columns n2 = 32*rank + c
+  {
+    const int c = threadIdx.x % kColsPerCta, j = threadIdx.x / kColsPerCta;
+    const int n2 = rank * kColsPerCta + c;
+    Tile t{tile, lp1};
+    cpx v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) v[r] = big_pre(mp, it, job, LG, int64_t(kN2) * (j + r * TPT1) + n2);
+    run_passes<N1, R1, 1>(v, j, c, t, mp.tw[log2c(N1)]);
+    // v[r] = output k1 = j + r*TPT1; twiddle w_L^(n2 k1)
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+      const int64_t g = int64_t(n2) * (j + r * TPT1);
+      v[r] = cmul(v[r], cmul(ldg(mp.sthi[LG] + (g >> lobits)), ldg(mp.stlo[LG] + (g & lomask))));
+    }
+    __syncthreads();
+    scatter_natural<N1, R1>(v, j, c, t);
+  }
+  cl.sync();
+
+  // ---- step 2: DFTs over n2 of the rows k1 = rank*K1 + kk
+  const int kk = threadIdx.x % K1, j2 = threadIdx.x / K1;
+  const int k1 = rank * K1 + kk;
+  cpx v[R2];
+#pragma unroll
+  for (int r = 0; r < R2; ++r) {
+    const int n2 = j2 + r * TPT2;
+    const cpx* src = cl.map_shared_rank(tile, n2 / kColsPerCta);
+    v[r] = src[(n2 % kColsPerCta) * lp1 + pad16(k1)];
+  }
+  cl.sync();  // every remote read of this CTA's tile is done
+  Tile t2{tile, lp2};
+  run_passes<kN2, R2, 1>(v, j2, kk, t2, mp.tw[log2c(kN2)]);
+  // v[r] = z_k, k = k1 + N1*k2, k2 = j2 + r*TPT2
+  if (it.combo == K_R2C || it.combo == K_DCT2) {
+    __syncthreads();
+    scatter_natural<kN2, R2>(v, j2, kk, t2);
+    cl.sync();
+#pragma unroll
+    for (int r = 0; r < R2; ++r) {
+      const int k2 = j2 + r * TPT2;
+      const int64_t k = int64_t(k1) + int64_t(N1) * k2;
+      if (2 * k > L) continue;
+      cpx zb = czero();
+      if (k != 0 && 2 * k != L) {
+        const int pk1 = k1 == 0 ? 0 : N1 - k1;
+        const int pk2 = k1 == 0 ? kN2 - k2 : kN2 - 1 - k2;
+        const cpx* src = cl.map_shared_rank(tile, pk1 / K1);
+        zb = src[(pk1 % K1) * lp2 + pad16(pk2)];
+      }
+      big_post_pair(mp, it, job, LG, k, v[r], zb);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < R2; ++r) big_post_single(mp, it, job, LG, int64_t(k1) + int64_t(N1) * (j2 + r * TPT2), v[r]);
+  }
+  cl.sync();  // the tile and the item slot may be reused
+}
+
+// Shared memory a CTA needs for its part of a long item.
+__host__ __device__ inline size_t cluster_big_smem() {
+  size_t m = 0;
+  for (int lg = 14; lg <= kBigMaxLog2L; ++lg) {
+    const int N1 = (1 << lg) / kN2, R1 = N1 / (kThreads / kColsPerCta);
+    const int K1 = N1 / kCluster, R2 = kN2 / (kThreads / K1);
+    const size_t a = size_t(kColsPerCta) * tile_pitch(N1, R1, kColsPerCta, 1) * sizeof(cpx);
+    const size_t b = size_t(K1) * tile_pitch(kN2, R2, K1, 1) * sizeof(cpx);
+    m = m > a ? m : a;
+    m = m > b ? m : b;
+  }
+  return kOffsetsBytes + 16 * ((m + 15) / 16);
+}
+
+// The persistent kernel in cluster form: long items first, each on a whole
+// cluster (cluster rank 0 takes the next one from counter[1] and the others
+// read its index through distributed shared memory), then every CTA takes
+// short items from counter[0] on its own.
+__global__ void __launch_bounds__(kThreads, MinBlocks<16>::value) mixed_cluster_kernel(const __grid_constant__ Params mp) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_item;
+  cg::cluster_group cl = cg::this_cluster();
+  for (;;) {
+    if (cl.block_rank() == 0 && threadIdx.x == 0) s_item = int(atomicAdd(mp.counter + 1, 1u));
+    cl.sync();
+    const int idx = *cl.map_shared_rank(&s_item, 0);
+    if (idx >= mp.nbig) break;
+    const Item it = mp.items[idx];
+    switch (it.log2L) {
+      case 14: run_cluster_big<14>(mp, it, smem); break;
+      case 15: run_cluster_big<15>(mp, it, smem); break;
+      default: run_cluster_big<16>(mp, it, smem); break;
+    }
+  }
+  cl.sync();  // rank 0's slot has been read by all before anyone moves on
+  for (;;) {
+    if (threadIdx.x == 0) s_item = mp.nbig + int(atomicAdd(mp.counter, 1u));
+    __syncthreads();
+    const int idx = s_item;
+    __syncthreads();
+    if (idx >= mp.nitems) break;
+    const Item it = mp.items[idx];
+    if (it.combo < 0) {
+      run_unit(mp, it);
+    } else {
+      switch (it.combo) {
+        case K_CPLX: run_small_any<LoadCplx, StoreCplx>(mp, it, smem); break;
+        case K_R2C: run_small_any<LoadR2C, StoreR2C>(mp, it, smem); break;
+        case K_C2R: run_small_any<LoadC2R, StoreC2R>(mp, it, smem); break;
+        case K_DCT2: run_small_any<LoadDCT2, StoreDCT2>(mp, it, smem); break;
+        case K_DCT3: run_small_any<LoadDCT3, StoreDCT3>(mp, it, smem); break;
+        default: run_small_any<LoadT4, StoreT4>(mp, it, smem); break;
+      }
+    }
+    __syncthreads();
+  }
+  cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
 // shared memory of the kernel: offsets + the largest tile of any item
 size_t kernel_smem() {
   size_t m = 0;
@@ -412,6 +706,7 @@ struct minfft_b200_mixed {
   int per_sm = 1;
   size_t smem = 0;
   int split = 1;  // jobs per short item = slots / split
+  bool cluster = false;  // long items on clusters (mixed_cluster_kernel)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -514,8 +809,14 @@ bool build_items(minfft_b200_mixed* m) {
     }
   }
   std::stable_sort(its.begin(), its.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  // long items first (the cluster form takes them from their own queue)
+  std::stable_partition(its.begin(), its.end(), [](const auto& a) { return a.second.big != 0; });
   m->items.clear();
-  for (auto& p : its) m->items.push_back(p.second);
+  int nbig = 0;
+  for (auto& p : its) {
+    m->items.push_back(p.second);
+    nbig += p.second.big ? 1 : 0;
+  }
   if (m->d_order) cudaFree(m->d_order);
   if (m->d_items) cudaFree(m->d_items);
   m->d_order = m->d_items = nullptr;
@@ -533,15 +834,32 @@ bool build_items(minfft_b200_mixed* m) {
   m->params.order = static_cast<const int*>(m->d_order);
   m->params.items = static_cast<const Item*>(m->d_items);
   m->params.nitems = int(m->items.size());
+  m->params.nbig = m->cluster ? nbig : 0;
   // graph: reset the queue counter, run the persistent kernel
   release_graph(m);
   cudaStream_t cs;
   if (!ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
   bool good = ok(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
   if (good) {
-    cudaMemsetAsync(m->d_counter, 0, sizeof(unsigned), cs);
+    cudaMemsetAsync(m->d_counter, 0, 2 * sizeof(unsigned), cs);
     void* args[1] = {&m->params};
-    cudaLaunchKernel((const void*)mixed_kernel, dim3(m->grid), dim3(kThreads), args, m->smem, cs);
+    if (m->cluster) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(m->grid);
+      cfg.blockDim = dim3(kThreads);
+      cfg.dynamicSmemBytes = m->smem;
+      cfg.stream = cs;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = kCluster;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      cudaLaunchKernelExC(&cfg, (const void*)mixed_cluster_kernel, args);
+    } else {
+      cudaLaunchKernel((const void*)mixed_kernel, dim3(m->grid), dim3(kThreads), args, m->smem, cs);
+    }
     good = ok(cudaStreamEndCapture(cs, &m->graph), "cudaStreamEndCapture");
   }
   if (good) good = ok(cudaGraphInstantiate(&m->exec, m->graph, 0), "cudaGraphInstantiate");
@@ -655,11 +973,42 @@ MB_EXPORT minfft_b200_mixed* minfft_b200_mixed_plan(int count, const minfft_b200
               "occupancy query");
   m->per_sm = std::max(1, occ);
   m->grid = sms * m->per_sm;
+  // long items: the cluster form where the device can co-schedule clusters
+  // of eight CTAs with this shared memory (MINFFT_B200_MIXED_CLUSTER=0 turns
+  // it off)
+  const char* ce = getenv("MINFFT_B200_MIXED_CLUSTER");
+  if (good && max_big > 0 && !(ce && ce[0] == '0')) {
+    const size_t csmem = std::max(kernel_smem(), cluster_big_smem());
+    int nclusters = 0;
+    if (cudaFuncSetAttribute((const void*)mixed_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(csmem)) == cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(kCluster);
+      cfg.blockDim = dim3(kThreads);
+      cfg.dynamicSmemBytes = csmem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = kCluster;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      if (cudaOccupancyMaxActiveClusters(&nclusters, (const void*)mixed_cluster_kernel, &cfg) != cudaSuccess)
+        nclusters = 0;
+    }
+    cudaGetLastError();
+    if (nclusters > 0) {
+      m->cluster = true;
+      m->smem = csmem;
+      m->grid = nclusters * kCluster;
+      m->per_sm = std::max(1, m->grid / sms);
+    }
+  }
   if (good) good = ok(mb::dev_malloc(&m->d_jobs, count * sizeof(Job)), "cudaMalloc(jobs)");
   if (good)
     good = ok(cudaMemcpy(m->d_jobs, m->jobs.data(), count * sizeof(Job), cudaMemcpyHostToDevice), "cudaMemcpy(jobs)");
-  if (good) good = ok(mb::dev_malloc(&m->d_counter, sizeof(unsigned)), "cudaMalloc(counter)");
-  if (good && max_big > 0) {
+  if (good) good = ok(mb::dev_malloc(&m->d_counter, 2 * sizeof(unsigned)), "cudaMalloc(counter)");
+  if (good && max_big > 0 && !m->cluster) {
     P.scratch_stride = int64_t(2) << kBigMaxLog2L;
     good = ok(mb::dev_malloc(&m->d_scratch, size_t(m->grid) * P.scratch_stride * sizeof(cpx)), "cudaMalloc(scratch)");
   }
@@ -703,6 +1052,7 @@ MB_EXPORT int minfft_b200_mixed_autotune(minfft_b200_mixed* m, int reps) {
     for (int per = 1; per <= max_per_sm; ++per) {
       m->split = split;
       m->grid = std::min(grid_cap, sms * per);
+      if (m->cluster) m->grid = std::max(kCluster, m->grid / kCluster * kCluster);
       if (!build_items(m)) continue;
       cudaGraphLaunch(m->exec, st);
       cudaEventRecord(e0, st);
@@ -722,5 +1072,6 @@ MB_EXPORT int minfft_b200_mixed_autotune(minfft_b200_mixed* m, int reps) {
   cudaStreamDestroy(st);
   m->split = best_split;
   m->grid = std::min(grid_cap, sms * best_per);
+  if (m->cluster) m->grid = std::max(kCluster, m->grid / kCluster * kCluster);
   return build_items(m) ? MINFFT_B200_OK : MINFFT_B200_ECUDA;
 }
