@@ -14,10 +14,12 @@ Other workloads (``--workload``): "batch4096" (1024 complex DFTs of length
 4096, c128, forward then inverse; 5 N log2 N per transform), "mixed20000"
 (20000 1-D transforms of mixed kinds and lengths in one persistent launch),
 "3d256" (256^3 c64 DFT, forward then inverse), "long1d" (2^26-point DFTs in
-c128 and c64, 2^24-point DCT-4/DST-4 in f64 and f32) and "long1d_c64" (the
-2^26-point c64 DFT, forward then inverse).  "3d256" and "long1d_c64" take
+c128 and c64, 2^24-point DCT-4/DST-4 in f64 and f32), "long1d_c64" (the
+2^26-point c64 DFT, forward then inverse) and "long1d_t4" (DCT-4 and DST-4
+of 2^24 points in f32).  "3d256", "long1d_c64" and "long1d_t4" take
 ``--precision fp32|tc_f16|tc_bf16`` (CUDA-core or tensor-core split-precision
-256-point passes).
+256-point passes).  The default run also measures every other workload
+briefly after the headline and reports them under "configs" (one GPU).
 
 Timing: W untimed warm-up steps, then exactly K steps between CUDA events on
 the stream the kernels run on (the legacy default stream), bracketed by a
@@ -97,6 +99,24 @@ def uniform_c64(dims, seed):
 
 
 _oracle_cache = {}
+
+
+def uniform_f32(dims, seed):
+    """i.i.d. uniform[-1,1) from numpy PCG64(seed), as float32 (kept for the other precisions)."""
+    key = ("f32", tuple(dims), seed)
+    if key not in _input_cache:
+        _input_cache[key] = np.random.default_rng(seed).uniform(-1, 1, dims).astype(np.float32)
+    return _input_cache[key]
+
+
+def oracle_real(name, seed, op, x, dims):
+    """The checker: the FP64 oracle's real transform `op` of x upcast, cached."""
+    key = (name, seed, op, tuple(dims))
+    if key not in _oracle_cache:
+        import oracle
+
+        _oracle_cache[key] = oracle.apply(op, x.astype(np.float64), dims, single=False, kind=oracle.best_kind())
+    return _oracle_cache[key]
 
 
 def oracle_kind_name():
@@ -900,8 +920,106 @@ class WorkloadLong1DC64(Workload3D256):
         return t, 5.0 * n * math.log2(n) * 2 * P * reps
 
 
+class WorkloadLong1DT4:
+    """DCT-4 and DST-4 of 2^24 points in f32: a pre-rotation, the 2^23-point
+    complex chain over HBM and a post-rotation.  --precision "tc_f16" /
+    "tc_bf16" runs the chain as two 256-point tensor-core passes and one
+    128-point CUDA-core pass; "fp32" as two 2048/4096-point CUDA-core passes."""
+
+    name = "long1d_t4"
+    dims = (1 << 24,)
+    nsets = 3
+    seed = 6
+    dtype = "f32"
+    precision = "fp32"
+
+    def __init__(self, torch, dev):
+        import minfft_b200
+
+        self.torch = torch
+        n = self.dims[0]
+        self.flops_per_transform = 2.5 * n * math.log2(n)
+        self.ops_per_step = 2
+        self.eng = minfft_b200.engine(True)
+        self.xs = [torch.from_numpy(uniform_f32(self.dims, self.seed + i)).to(dev) for i in range(self.nsets)]
+        self.c = torch.empty(self.dims, dtype=torch.float32, device=dev)
+        self.s = torch.empty(self.dims, dtype=torch.float32, device=dev)
+        self.plan = self._mkplan()
+        self.plan("dct4", self.xs[0].data_ptr(), self.c.data_ptr())
+        self.plan("dst4", self.xs[0].data_ptr(), self.s.data_ptr())
+        torch.cuda.synchronize()
+        self.eng.tc_status(self.plan.aux)
+        x = self.xs[0].cpu().numpy()
+        acc = {}
+        for op, y in (("dct4", self.c), ("dst4", self.s)):
+            ref = oracle_real(self.name, self.seed, op, x, self.dims)
+            acc[f"{op}_rel_l2_vs_fp64_oracle"] = float(np.linalg.norm(y.cpu().numpy().astype(np.float64) - ref) /
+                                                       np.linalg.norm(ref))
+        acc["oracle"] = oracle_kind_name()
+        self.accuracy = acc
+
+    def _mkplan(self):
+        plan = self.eng.plan("t4", self.dims)
+        self.eng.set_precision(plan.aux, self.precision)
+        return plan
+
+    def plans(self):
+        yield self.eng, self.plan, ("dct4", "dst4")
+
+    def rebuild(self, eng, plan):
+        self.plan.free()
+        self.plan = self._mkplan()
+
+    def step(self, k):
+        x = self.xs[k % self.nsets]
+        self.plan("dct4", x.data_ptr(), self.c.data_ptr(), check=False)
+        self.plan("dst4", x.data_ptr(), self.s.data_ptr(), check=False)
+
+    def check_errors(self):
+        self.eng.check()
+        self.eng.tc_status(self.plan.aux)
+
+    def launches_per_step(self):
+        return sum(self.eng.launch_count(op, self.plan.aux) for op in ("dct4", "dst4"))
+
+    def e2e_setup(self):
+        t = self.torch
+        self.hx = t.empty(self.dims, dtype=t.float32, pin_memory=True)
+        self.hx.copy_(self.xs[0].cpu())
+        self.e2e_sets = alternate_plan_sets(t, [self.plan, self._mkplan()], self.hx, 2)
+        self.e2e_k = 0
+        b = self.hx.numel() * 4
+        return 2 * b, 2 * b
+
+    def e2e_step(self):
+        plan, (hc, hs) = next_plan_set(self)
+        plan("dct4", self.hx.data_ptr(), hc.data_ptr(), check=False)
+        plan("dst4", self.hx.data_ptr(), hs.data_ptr(), check=False)
+
+    @classmethod
+    def config(cls):
+        return {"workload": "1-D DCT-4 + DST-4 N=2^24 f32", "dims": list(cls.dims), "precision": cls.precision,
+                "flops": "2.5*N*log2(N) per transform, N=2^24",
+                "inputs": "i.i.d. uniform[-1,1), numpy PCG64 seeds 6..8",
+                "l2": "inputs rotate over 3 sets of 64 MiB; each step writes 128 MiB, beyond the 126 MB L2"}
+
+    cpu_sequences = (("t4", ("dct4", "dst4"), True),)
+
+    @classmethod
+    def cpu_sample(cls, P):
+        return f"{min(P, 8)} concurrent instances (one per OpenMP thread, own plans) of dct4 + dst4, per timed step"
+
+    @classmethod
+    def cpu_measure(cls, kind, threads, warm, reps):
+        P = min(threads, 8)
+        t = cpu_run(kind, cls.cpu_sequences, cls.dims, P, P, reps, warm)
+        n = cls.dims[0]
+        return t, 2.5 * n * math.log2(n) * 2 * P * reps
+
+
 WORKLOADS = {"2d2048": Workload2D, "batch4096": WorkloadBatch4096, "mixed20000": WorkloadMixed,
-             "3d256": Workload3D256, "long1d": WorkloadLong1D, "long1d_c64": WorkloadLong1DC64}
+             "3d256": Workload3D256, "long1d": WorkloadLong1D, "long1d_c64": WorkloadLong1DC64,
+             "long1d_t4": WorkloadLong1DT4}
 
 
 # -------------------------------------------------------------- CPU timing
@@ -1176,7 +1294,9 @@ SUB_CONFIGS = (("batch4096", "batch4096", None),
                ("mixed20000", "mixed20000", None),
                ("long1d", "long1d", None),
                ("long1d_c64_fp32", "long1d_c64", "fp32"), ("long1d_c64_tc_f16", "long1d_c64", "tc_f16"),
-               ("long1d_c64_tc_bf16", "long1d_c64", "tc_bf16"))
+               ("long1d_c64_tc_bf16", "long1d_c64", "tc_bf16"),
+               ("long1d_t4_fp32", "long1d_t4", "fp32"), ("long1d_t4_tc_f16", "long1d_t4", "tc_f16"),
+               ("long1d_t4_tc_bf16", "long1d_t4", "tc_bf16"))
 
 
 def single_thread_reference():
@@ -1297,7 +1417,7 @@ def main():
                     help="skip the short runs of the other workloads after the default headline")
     ap.add_argument("--sub-steps", type=int, default=10, help="timed steps of each other workload")
     ap.add_argument("--precision", choices=["fp32", "tc_f16", "tc_bf16"], default="fp32",
-                    help="3d256, long1d_c64: arithmetic of the 256-point axis passes")
+                    help="3d256, long1d_c64, long1d_t4: arithmetic of the 256-point axis passes")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

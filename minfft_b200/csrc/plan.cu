@@ -1260,8 +1260,19 @@ struct Planner {
   // Stockham FFT over HBM for a long axis (see the file comment).
   void plan_multipass(const AxisStep& s, int64_t Lt) {
     const int bits = ilog2(Lt);
-    const int P = (bits + kPassCapLog2 - 1) / kPassCapLog2;
-    const std::vector<int> pb = pass_bits(bits, P);
+    int P = (bits + kPassCapLog2 - 1) / kPassCapLog2;
+    std::vector<int> pb = pass_bits(bits, P);
+    // a tensor-core mode whose chain has no 256-point pass at the FP32 pass
+    // count (2^17 .. 2^24 points in two passes) takes one more pass so that
+    // its radix-16 stages run on the tensor cores
+    if (a->precision != MINFFT_B200_PREC_FP32 && bits >= 2 * ilog2(mb::kTcLength) &&
+        std::find(pb.begin(), pb.end(), ilog2(mb::kTcLength)) == pb.end()) {
+      std::vector<int> more = pass_bits(bits, P + 1);
+      if (std::find(more.begin(), more.end(), ilog2(mb::kTcLength)) != more.end()) {
+        pb = more;
+        P = P + 1;
+      }
+    }
     const int64_t inner = s.inner, outer = s.outer;
     const int64_t Lp = Lt * inner;
     const size_t work_bytes = size_t(outer) * size_t(Lp) * sizeof(cpx);

@@ -53,6 +53,14 @@ def run_mode(family, op, x, dims, mode):
     plan = eng.plan(family, dims)
     try:
         eng.set_precision(plan.aux, mode)
+        if mode != "fp32":  # the tensor-core passes do run
+            eng.profile(plan.aux, 1)
+            probe = torch.zeros(2 * int(np.prod(dims)) + 8, dtype=torch.float32, device="cuda")
+            out = torch.zeros_like(probe)
+            plan(op, probe.data_ptr(), out.data_ptr())
+            labels = [s[0] for s in eng.profile_stats(plan.aux)]
+            eng.profile(plan.aux, 0)
+            assert any(lab.startswith(("tc_pass<", "tc_stream<")) for lab in labels), labels
         xt = torch.from_numpy(np.ascontiguousarray(x)).cuda()
         _, _, out_shape, out_c = shapes(op, dims)
         y = torch.full(out_shape, float("nan"), dtype=torch.complex64 if out_c else torch.float32, device="cuda")
