@@ -529,7 +529,9 @@ struct Planner {
 
   // Form of the tensor-core pass: the streamed form (tc_stream_kernel) by
   // default, the one-tile form with MINFFT_B200_TC_FORM=tile; stages of the
-  // streamed form from MINFFT_B200_TC_STAGES (2 .. 6, default 3).
+  // streamed form from MINFFT_B200_TC_STAGES (2 .. 6; default 2 for FP16,
+  // which then fits two CTAs per SM, and 3 for BF16, whose larger operands
+  // allow one).
   static bool tc_stream_default() {
     static const bool on = [] {
       const char* e = getenv("MINFFT_B200_TC_FORM");
@@ -537,13 +539,13 @@ struct Planner {
     }();
     return on;
   }
-  static int tc_stream_stages() {
+  static int tc_stream_stages(int fmt) {
     static const int n = [] {
       const char* e = getenv("MINFFT_B200_TC_STAGES");
-      const int v = e ? atoi(e) : 3;
-      return v < 2 ? 2 : (v > 6 ? 6 : v);
+      const int v = e ? atoi(e) : 0;
+      return v <= 0 ? 0 : (v < 2 ? 2 : (v > 6 ? 6 : v));
     }();
-    return n;
+    return n ? n : (fmt == mb::TC_F16 ? 2 : 3);
   }
 
   // Normalised layout of the streamed tensor-core pass: b0 indexes the
@@ -570,7 +572,7 @@ struct Planner {
     if (!tc_stream_default() || L != mb::kTcLength || !tc_stream_normalise(nbatch, ap)) return false;
     if (!ap.colmode && (ap.flags & mb::F_STAGE_ROWS)) return false;
     const bool rows = !ap.colmode;
-    const int stages = tc_stream_stages();
+    const int stages = tc_stream_stages(fmt);
     Launch ln;
     ln.key = key;
     ln.radix = 16;

@@ -663,7 +663,7 @@ __device__ __forceinline__ void tcs_read_d(uint32_t tmem, int warp, float (&re)[
 }
 
 template <int FMT, bool ROWS>
-__global__ void __launch_bounds__(kTcsNT, 1) tc_stream_kernel(const AxisParams p, const TcParams q,
+__global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kernel(const AxisParams p, const TcParams q,
                                                               const __grid_constant__ CUtensorMap tmap) {
   using Lay = TcsLayout<FMT>;
   constexpr int NT = Lay::NT;
