@@ -80,6 +80,11 @@ struct AxisParams {
   int stage_bytes;      // pipelined kernel: bytes of one shared-memory stage
   int lp;               // shared-memory pitch between transforms (tile_pitch)
   int* status;          // set to 1 by a kernel whose bounded device-side wait ran out
+  // type-4 steps fused into the first / last pass of a 1-D chain over HBM:
+  // real length N of the line, reals between lines of the real input /
+  // output, and the fine-table bits of the post-rotation roots (t1, t2)
+  int64_t kn, k_in_line, k_out_line;
+  int kbits;
 };
 
 enum : int {
@@ -704,6 +709,46 @@ struct LoadDCT3 {
   }
 };
 
+// Type-4 pre-rotation fused into the first pass of a Stockham chain over
+// HBM along a 1-D line (reference minfft.c:906-910, 953-957).  Element n of
+// sub-DFT b (b1 = its index in the line, b2 = the line) is the line's
+// complex point g = b1 + n*in_n: t_g = w_2N^g (x[2g] + i x[N-1-2g]) for
+// DCT-4, -w_2N^g (x[2g] - i x[N-1-2g]) for DST-4, x the line's N = kn reals
+// at b2 * k_in_line.  w_2N^g is the product of the coarse and fine roots
+// (st_hi, st_lo, st_lobits) of 2N: the first pass has no pre-twiddle of its
+// own.  Each real is read once overall: x[2g] here, its neighbour x[2g+1]
+// by element N/2-1-g.
+struct LoadT4Chain {
+  static constexpr bool kStaged = false;
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+    constexpr int TPT = L / R;
+    if (!x.active) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = czero();
+      return;
+    }
+    const int64_t rest = x.b / p.d0;
+    const int64_t b1 = rest % p.d1, b2 = rest / p.d1;
+    const real* in = static_cast<const real*>(p.in) + b2 * p.k_in_line;
+    const int64_t N = p.kn;
+    const bool dst = (p.flags & F_DST) != 0;
+    const int64_t lomask = (int64_t(1) << p.st_lobits) - 1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t g = b1 * p.is1 + int64_t(x.j + r * TPT) * p.in_n;
+      const real a = in[2 * g], b = in[N - 1 - 2 * g];
+      const cpx e = cmul(ldg(p.st_hi + (g >> p.st_lobits)), ldg(p.st_lo + (g & lomask)));
+      if (!dst) {
+        v[r] = cmul(e, cmk(a, b));
+      } else {
+        const cpx q = cmul(e, cmk(a, -b));
+        v[r] = cmk(-q.x, -q.y);
+      }
+    }
+  }
+};
+
 // --------------------------------------------------------------- store ops
 // Each store op receives output element k = j + r*(L/R) of the length-L DFT
 // in v[r].
@@ -997,6 +1042,40 @@ struct StoreT4 {
       const cpx b = cmul(cmulc(ghi, w128(r * (32 / R))), cconj(T));
       lo[r * st] = 2 * (dst ? a.y : a.x);
       hi[-r * st] = 2 * (dst ? b.y : b.x);
+    }
+  }
+};
+
+// Type-4 post-rotation fused into the last pass of a Stockham chain over
+// HBM along a 1-D line (reference minfft.c:916-921, 963-968): output k of
+// sub-DFT b is the line's point m = (its normal offset) + k*out_k, and
+// T_m gives y[2m] = 2 Re(g_2m T_m), y[N-1-2m] = 2 Re(g_{N-1-2m} conj(T_m))
+// (Im for DST-4), g_q = w_8N^(2q+1) as the product of the coarse and fine
+// roots t1, t2 of 8N (kbits fine bits); y is the line's N reals at
+// b2 * k_out_line (the pass's os2 is 0).
+struct StoreT4Chain {
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, const TileOffsets&,
+                                             cpx (&v)[R]) {
+    if (!x.active) return;
+    constexpr int TPT = L / R;
+    const int64_t b2 = x.b / (p.d0 * p.d1);
+    real* out = static_cast<real*>(p.out) + b2 * p.k_out_line;
+    const int64_t N = p.kn;
+    const bool dst = (p.flags & F_DST) != 0;
+    const int64_t lomask = (int64_t(1) << p.kbits) - 1;
+    auto g = [&](int64_t q) {
+      const int64_t e = 2 * q + 1;
+      return cmul(ldg(p.t1 + (e >> p.kbits)), ldg(p.t2 + (e & lomask)));
+    };
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t m = x.oout + int64_t(x.j + r * TPT) * p.out_k;
+      const cpx T = v[r];
+      const cpx a = cmul(g(2 * m), T);
+      const cpx b = cmul(g(N - 1 - 2 * m), cconj(T));
+      out[2 * m] = 2 * (dst ? a.y : a.x);
+      out[N - 1 - 2 * m] = 2 * (dst ? b.y : b.x);
     }
   }
 };

@@ -15,6 +15,8 @@ const void* axis_kernel_dct3(int log2L, int radix16);
 const void* axis_kernel_t4(int log2L, int radix16);
 const void* axis_kernel_r2cq(int log2L, int radix16);
 const void* axis_kernel_c2rq(int log2L, int radix16);
+const void* axis_kernel_t4in(int log2L, int radix16);
+const void* axis_kernel_t4out(int log2L, int radix16);
 
 const void* pipe_kernel_cplx(int log2L, int radix16);
 const void* pipe_kernel_r2c(int log2L, int radix16);
@@ -58,6 +60,8 @@ const void* axis_kernel(int combo, int log2L, int R) {
     case K_T4: return axis_kernel_t4(log2L, R >= 16);
     case K_R2CQ: return axis_kernel_r2cq(log2L, R >= 16);
     case K_C2RQ: return axis_kernel_c2rq(log2L, R >= 16);
+    case K_T4IN: return axis_kernel_t4in(log2L, R >= 16);
+    case K_T4OUT: return axis_kernel_t4out(log2L, R >= 16);
     default: return nullptr;
   }
 }

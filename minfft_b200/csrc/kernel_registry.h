@@ -13,6 +13,8 @@ enum Combo : int {
   K_T4,         // DCT-4 / DST-4 with fused pre- and post-rotation
   K_R2CQ,       // real DFT of 4 rows j + Q*m, then the first radix-4 stage of the column DFT across them
   K_C2RQ,       // last radix-4 stage of an inverse column DFT across 4 rows, then their inverse real DFT
+  K_T4IN,       // first pass of a 1-D type-4 chain over HBM: the pre-rotation fused into its load
+  K_T4OUT,      // last pass of a 1-D type-4 chain over HBM: the post-rotation fused into its store
   K_COUNT
 };
 

@@ -895,7 +895,7 @@ MB_EXPORT minfft_b200_mixed* minfft_b200_mixed_plan(int count, const minfft_b200
   m->jobs.resize(count);
   int max_big = 0;
   std::vector<int> need_tw(kSlots, 0), need_n(kSlots, 0), need_st(kSlots, 0);
-  std::vector<int> need_kind(kSlots * 8, 0);
+  std::vector<int> need_kind(kSlots * mb::K_COUNT, 0);
   for (int i = 0; i < count; ++i) {
     const minfft_b200_job& j = jobs[i];
     const int64_t n = j.n;

@@ -508,6 +508,16 @@ struct Planner {
            (ap.flags & ~(mb::F_CONJ_IN | mb::F_CONJ_OUT | mb::F_STAGE_ROWS)) == 0;
   }
 
+  // Type-4 pre/post-rotations fused into the chain passes (MINFFT_B200_T4FUSE=0
+  // keeps them as separate element-wise kernels).
+  static bool t4_fuse_enabled() {
+    static const bool on = [] {
+      const char* e = getenv("MINFFT_B200_T4FUSE");
+      return !(e && e[0] == '0');
+    }();
+    return on;
+  }
+
   // Sub-DFT lengths (log2) of the P passes of a Stockham chain over
   // 2^bits points: as even as possible, the longer ones first; in a
   // tensor-core precision mode, as many 256-point passes (first) as the
@@ -798,17 +808,20 @@ struct Planner {
     ln.out_buf = out_buf;
     ln.vec_in = vec_in;
     ln.vec_out = vec_out;
-    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R || combo == mb::K_C2RQ);
-    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C || combo == mb::K_R2CQ);
+    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R || combo == mb::K_C2RQ || combo == mb::K_T4OUT);
+    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C || combo == mb::K_R2CQ || combo == mb::K_T4IN);
     ln.combo = combo;
     ln.L = L;
     ln.ap = ap;
     {
-      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4", "r2c+col4", "col4+c2r"};
+      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4", "r2c+col4", "col4+c2r",
+                                    "t4pre+cplx", "cplx+t4post"};
       const double R = sizeof(real), C = sizeof(cpx);
       double per = 0;
       switch (combo) {
         case mb::K_CPLX: per = 2.0 * L * C; break;
+        case mb::K_T4IN:
+        case mb::K_T4OUT: per = 2.0 * L * R + L * C; break;
         case mb::K_R2C:
         case mb::K_R2CQ: per = 2.0 * L * R + (L + 1) * C; break;
         case mb::K_C2R:
@@ -968,13 +981,14 @@ struct Planner {
     ln.in_buf = in_buf;
     ln.out_buf = out_buf;
     ln.vec_out = (combo == mb::K_C2R);
-    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R || combo == mb::K_C2RQ);
-    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C || combo == mb::K_R2CQ);
+    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R || combo == mb::K_C2RQ || combo == mb::K_T4OUT);
+    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C || combo == mb::K_R2CQ || combo == mb::K_T4IN);
     ln.combo = combo;
     ln.L = L;
     ln.ap = ap;
     {
-      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4", "r2c+col4", "col4+c2r"};
+      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4", "r2c+col4", "col4+c2r",
+                                    "t4pre+cplx", "cplx+t4post"};
       const double Rb = sizeof(real), C = sizeof(cpx);
       double per = 0;
       switch (combo) {
@@ -1295,7 +1309,13 @@ struct Planner {
       lp.flags = s.flags;
       return lp;
     };
-    if (s.combo == mb::K_DCT2 || s.combo == mb::K_T4 || s.combo == mb::K_C2R || s.combo == mb::K_DCT3) {
+    // A 1-D type-4 chain of two or more passes in FP32 fuses its pre-rotation
+    // into the first pass's load and its post-rotation into the last pass's
+    // store (LoadT4Chain, StoreT4Chain): two passes over HBM instead of four.
+    const bool t4_fused = s.combo == mb::K_T4 && inner == 1 && P >= 2 && a->precision == MINFFT_B200_PREC_FP32 &&
+                          t4_fuse_enabled();
+    if (!t4_fused &&
+        (s.combo == mb::K_DCT2 || s.combo == mb::K_T4 || s.combo == mb::K_C2R || s.combo == mb::K_DCT3)) {
       cs = BUF_T2;
       need(cs, work_bytes);
       LineParams lp = line(s.in_row, inner, Lp, inner);
@@ -1318,7 +1338,8 @@ struct Planner {
       }
       add_line_kernel(which, lp, items, s.in_buf, cs);
     }
-    const bool post = (s.combo == mb::K_R2C || s.combo == mb::K_DCT2 || s.combo == mb::K_DCT3 || s.combo == mb::K_T4);
+    const bool post =
+        !t4_fused && (s.combo == mb::K_R2C || s.combo == mb::K_DCT2 || s.combo == mb::K_DCT3 || s.combo == mb::K_T4);
 
     // --- the HBM passes
     int prev = cs;
@@ -1338,6 +1359,7 @@ struct Planner {
       } else {
         dst = s.out_buf;
       }
+      const bool fuse_in = t4_fused && p == 0, fuse_out = t4_fused && last;
       const int64_t Nsp = Ns * inner;
       AxisParams ap = base_params();
       ap.d0 = Nsp;
@@ -1365,7 +1387,28 @@ struct Planner {
       if (p == 0 && inverse_cplx) ap.flags |= mb::F_CONJ_IN;
       if (last && conj_chain && s.combo != mb::K_DCT3) ap.flags |= mb::F_CONJ_OUT;
       ap.tw = tab(TB_TW, Rp);
-      add_axis_kernel(mb::K_CPLX, (int)Rp, outer * (Lp / Rp), ap, prev, dst, false, false);
+      int combo = mb::K_CPLX;
+      if (fuse_in) {
+        combo = mb::K_T4IN;
+        ap.flags |= (s.flags & mb::F_DST);
+        ap.st_hi = tab(TB_STHI, 2 * s.N);  // w_2N^g, coarse x fine
+        ap.st_lo = tab(TB_STLO, 2 * s.N);
+        ap.st_lobits = (int)st_lobits_for(2 * s.N);
+        ap.is2 = 0;
+        ap.kn = s.N;
+        ap.k_in_line = s.in_row;
+      }
+      if (fuse_out) {
+        combo = mb::K_T4OUT;
+        ap.flags |= (s.flags & mb::F_DST);
+        ap.t1 = tab(TB_STHI, 8 * s.N);  // w_8N^(2q+1), coarse x fine
+        ap.t2 = tab(TB_STLO, 8 * s.N);
+        ap.kbits = (int)st_lobits_for(8 * s.N);
+        ap.os2 = 0;
+        ap.kn = s.N;
+        ap.k_out_line = s.out_row;
+      }
+      add_axis_kernel(combo, (int)Rp, outer * (Lp / Rp), ap, prev, dst, false, false);
       if (ok) prog->launches.back().hbm_pass = true;
       prev = dst;
       Ns *= Rp;
@@ -2185,6 +2228,18 @@ Extent launch_extent(const Launch& ln) {
         e.in_max = oi + L * ap.in_n;
         e.out_max = oo + 2 * L - 1;
         break;
+      case mb::K_T4IN: {  // the real lines of the input (the pass's is2 is 0)
+        const int64_t lines = ap.nbatch / (ap.d0 * ap.d1);
+        e.in_max = (lines - 1) * ap.k_in_line + ap.kn - 1;
+        e.out_max = oo + (L - 1) * ap.out_k;
+        break;
+      }
+      case mb::K_T4OUT: {  // the real lines of the output (the pass's os2 is 0)
+        const int64_t lines = ap.nbatch / (ap.d0 * ap.d1);
+        e.in_max = oi + (L - 1) * ap.in_n;
+        e.out_max = (lines - 1) * ap.k_out_line + ap.kn - 1;
+        break;
+      }
       default:
         e.in_max = oi + (2 * L - 1) * ap.in_n;
         e.out_max = oo + (2 * L - 1) * ap.out_k;

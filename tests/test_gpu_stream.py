@@ -83,3 +83,24 @@ def test_streamed_pass_with_offset_input(single):
         assert err <= tolerance(single, dims)
     finally:
         eng.tune_set_default(-1, 0, 16)
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+def test_fused_type4_chain_matches_oracle(single):
+    """1-D DCT-4 / DST-4 lines longer than one CTA run their pre-rotation in
+    the first pass over HBM and their post-rotation in the last one
+    (LoadT4Chain, StoreT4Chain): single lines, several lines of a 2-D array,
+    and in-place calls, against the oracle."""
+    eng = minfft_b200.engine(single)
+    rng = np.random.default_rng(63)
+    for dims in [(1 << 15,), (1 << 18,), (3, 1 << 16)]:
+        plan_labels = labels(eng, "dct4", dims)
+        assert any("t4pre" in lab for lab in plan_labels), plan_labels
+        for op in ("dct4", "dst4"):
+            x = make_input(op, dims, rng, single)
+            err = rel_l2(gpu_apply(op, x, dims, single), expected(op, x, dims))
+            assert err <= tolerance(single, dims), (op, dims, err)
+    dims = (1 << 16,)
+    x = make_input("dst4", dims, rng, single)
+    err = rel_l2(gpu_apply("dst4", x, dims, single, inplace=True), expected("dst4", x, dims))
+    assert err <= tolerance(single, dims)

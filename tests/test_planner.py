@@ -130,7 +130,10 @@ def test_tensor_core_plans_are_in_bounds(dims, precision):
             bad, rep, n = eng.plan_selfcheck(op, dims, howmany, alias, precision=precision)
             assert bad == 0, f"{op} {dims} {precision} howmany={howmany} alias={alias}:\n{rep}"
             _, _, n32 = eng.plan_selfcheck(op, dims, howmany, alias)
-            assert n in (n32, n32 + 1)
+            # FP32 fuses the type-4 rotations of a 1-D chain into its first and
+            # last passes; the tensor-core chains keep them as element-wise steps
+            extra = 2 if op in ("dct4", "dst4") else 0
+            assert n32 <= n <= n32 + 1 + extra
 
 
 # (length, passes of its chain in a tensor-core mode: 256-point tensor-core
