@@ -85,6 +85,9 @@ struct AxisParams {
   // output, and the fine-table bits of the post-rotation roots (t1, t2)
   int64_t kn, k_in_line, k_out_line;
   int kbits;
+  // streamed row pass: stages in flight, bytes copied per row, bytes
+  // between rows of a stage
+  int nstages, row_bytes, row_pitch;
 };
 
 enum : int {
@@ -374,6 +377,7 @@ __device__ __forceinline__ void hbm_pretwiddle(cpx (&v)[R], const AxisParams& p,
 
 // Plain complex input; optional conjugation and large-length pre-twiddle.
 struct LoadCplx {
+  static constexpr bool kComplexIn = true;  // whether the raw input elements are complex
   static constexpr bool kStaged = false;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
@@ -403,6 +407,7 @@ struct LoadCplx {
 // Real row read as L complex pairs (x[2n], x[2n+1]): the half-length complex
 // DFT of the real DFT (reference minfft.c:541-543).
 struct LoadR2C {
+  static constexpr bool kComplexIn = false;  // whether the raw input elements are complex
   static constexpr bool kStaged = false;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
@@ -427,6 +432,7 @@ struct LoadR2C {
 // length-N sequence u_i = x[2i] (i < N/2), u_i = +-x[2N-1-2i] (i >= N/2)
 // read as complex pairs (u_2m, u_2m+1); N = 2L.
 struct LoadDCT2 {
+  static constexpr bool kComplexIn = false;  // whether the raw input elements are complex
   static constexpr bool kStaged = false;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
@@ -463,6 +469,7 @@ struct LoadDCT2 {
 // t_n = e_n (x[2n] + i x[N-1-2n]) for DCT-4, -e_n (x[2n] - i x[N-1-2n]) for
 // DST-4, with e_n = w_2N^n from table t1.
 struct LoadT4 {
+  static constexpr bool kComplexIn = false;  // whether the raw input elements are complex
   static constexpr bool kStaged = false;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
@@ -568,6 +575,7 @@ __device__ __forceinline__ void pack_into(const Tile& t, int c, int k, int L, cp
 // values, staged in shared memory.  Stored conjugated: the inverse DFT is
 // computed as conj(DFT(conj(t))).  t2 = w_N^k, k < L/2.
 struct LoadC2R {
+  static constexpr bool kComplexIn = true;  // whether the raw input elements are complex
   static constexpr bool kStaged = true;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
@@ -590,6 +598,7 @@ struct LoadC2R {
 // columns of the pair for every row and packs them (one root w_N^k for all
 // four).  t1 = w_Nr^n, t2 = w_N^k.
 struct LoadC2RQ {
+  static constexpr bool kComplexIn = true;  // whether the raw input elements are complex
   static constexpr bool kStaged = true;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
@@ -630,6 +639,7 @@ struct LoadC2RQ {
 // inverse-real-DFT packing, staged in shared memory (conjugated as above).
 // t1 = w_4N^n (n < N/2), t2 = w_N^k (k < L/2); N = 2L.
 struct LoadDCT3 {
+  static constexpr bool kComplexIn = false;  // whether the raw input elements are complex
   static constexpr bool kStaged = true;
   // z_n of the type-3 pre-rotation; rd(i) returns input real x_i
   template <class Rd>
@@ -719,6 +729,7 @@ struct LoadDCT3 {
 // own.  Each real is read once overall: x[2g] here, its neighbour x[2g+1]
 // by element N/2-1-g.
 struct LoadT4Chain {
+  static constexpr bool kComplexIn = false;  // whether the raw input elements are complex
   static constexpr bool kStaged = false;
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {

@@ -33,6 +33,10 @@ const void* pipe_kernel(int combo, int log2L, int R = 16);
 // radix R (16, or 8 where the CTA stays within 512 threads), or nullptr.
 const void* stream_kernel(int log2L, int R);
 
+// The streamed row pass (stream_pass.cuh) of kind `combo` for log2(L) = 6 ..
+// 12 (11 for the split-column kinds), radix 16, or nullptr.
+const void* stream_rows_kernel_fn(int combo, int log2L);
+
 // Root tables kept on the device by plans: w_N^m (m < N); the real-DFT
 // table w_N^k (k < N/4); the type-2/3 table w_4N^n (n < N/2); the type-4
 // tables w_2N^n (n < N/2) and w_8N^(2q+1) (q < N); and the coarse/fine pair

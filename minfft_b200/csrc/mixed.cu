@@ -973,11 +973,12 @@ MB_EXPORT minfft_b200_mixed* minfft_b200_mixed_plan(int count, const minfft_b200
               "occupancy query");
   m->per_sm = std::max(1, occ);
   m->grid = sms * m->per_sm;
-  // long items: the cluster form where the device can co-schedule clusters
-  // of eight CTAs with this shared memory (MINFFT_B200_MIXED_CLUSTER=0 turns
-  // it off)
+  // long items: the cluster form with MINFFT_B200_MIXED_CLUSTER=1, where the
+  // device can co-schedule clusters of eight CTAs with this shared memory
+  // (measured slower than the per-CTA scratch form on the 20000-job batch,
+  // so not the default)
   const char* ce = getenv("MINFFT_B200_MIXED_CLUSTER");
-  if (good && max_big > 0 && !(ce && ce[0] == '0')) {
+  if (good && max_big > 0 && ce && ce[0] == '1') {
     const size_t csmem = std::max(kernel_smem(), cluster_big_smem());
     int nclusters = 0;
     if (cudaFuncSetAttribute((const void*)mixed_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

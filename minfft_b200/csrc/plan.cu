@@ -255,6 +255,7 @@ struct Launch {
   bool hbm_pass = false; // a pass of the Stockham FFT over HBM (never in place)
   bool pipe = false;     // persistent pipelined kernel (pipe_pass.cuh)
   bool stream = false;   // persistent TMA-fed column pass (stream_pass.cuh)
+  bool stream_rows = false;  // persistent bulk-copy-fed row pass (stream_pass.cuh)
   int tcs = 0;           // tensor-core pass in streamed form: 1 column tiles, 2 row tiles
   int64_t st_d2 = 1;     // streamed pass: outermost batch extent of its tensor copies
   bool tc = false;       // tensor-core split-precision pass (tc_pass.cu)
@@ -737,6 +738,10 @@ struct Planner {
         add_stream_kernel(L, nbatch, ap, in_buf, out_buf, tv.cpb, key, tv.radix);
         return;
       }
+      if ((tv.pipe == 3 || tv.pipe == 4) && stream_rows_fits(combo, L, ap, tv.cpb, tv.pipe - 1)) {
+        add_stream_rows_kernel(combo, L, nbatch, ap, in_buf, out_buf, tv.cpb, tv.pipe - 1, key, vec_in, vec_out);
+        return;
+      }
       if (tv.pipe == 1 && pipe_fits(combo, L, tv.cpb, ap.colmode, tv.radix)) {
         add_pipe_kernel(combo, L, nbatch, ap, in_buf, out_buf, tv.cpb, key, tv.radix);
         return;
@@ -756,6 +761,14 @@ struct Planner {
       if (ov.pipe == 2 && stream_fits(combo, L, nbatch, ap, ov.radix, st_stages)) {
         add_stream_kernel(L, nbatch, ap, in_buf, out_buf, st_stages, key, ov.radix);
         return;
+      }
+      if ((ov.pipe == 3 || ov.pipe == 4) && L >= 64) {
+        int c = four_rows(combo) ? 4 : (ov.cpb > 0 ? ov.cpb : std::max(1, 256 / (L / 16)));
+        while (c > 1 && !stream_rows_fits(combo, L, ap, c, ov.pipe - 1) && !four_rows(combo)) c /= 2;
+        if (stream_rows_fits(combo, L, ap, c, ov.pipe - 1)) {
+          add_stream_rows_kernel(combo, L, nbatch, ap, in_buf, out_buf, c, ov.pipe - 1, key, vec_in, vec_out);
+          return;
+        }
       }
       if (want_pipe) {
         int pc = ov.cpb > 0 ? ov.cpb : choose_pipe_cpb(combo, L, ap.colmode != 0);
@@ -930,6 +943,95 @@ struct Planner {
     snprintf(buf, sizeof(buf), "stream_pass<cplx,L=%d,col%s> batch=%lld", L, ap.st_ns > 1 ? ",hbm" : "",
              (long long)nbatch);
     ln.label = buf;
+    prog->launches.push_back(ln);
+  }
+
+  // The streamed row pass: row-mode launches whose rows are contiguous,
+  // lengths 64 .. 4096 (2048 for the split-column kinds), cpb rows per tile
+  // and `stages` tiles in flight (tuning forms 3 and 4: two and three).
+  static int raw_row_elems(int combo, int L) {
+    switch (combo) {
+      case mb::K_CPLX: return L;
+      case mb::K_C2R:
+      case mb::K_C2RQ: return L + 1;
+      default: return 2 * L;
+    }
+  }
+  static int raw_elem_size(int combo) {
+    return (combo == mb::K_CPLX || combo == mb::K_C2R || combo == mb::K_C2RQ) ? int(sizeof(cpx)) : int(sizeof(real));
+  }
+  bool stream_rows_fits(int combo, int L, const AxisParams& ap, int cpb, int stages) const {
+    if (L < 64 || ap.colmode || ap.in_n != 1 || cpb < 1 || stages < 2 || stages > 8) return false;
+    if (four_rows(combo) && cpb != 4) return false;
+    if (!mb::stream_rows_kernel_fn(combo, ilog2(L)) || cpb * (L / 16) > 512) return false;
+    const int rb = raw_row_elems(combo, L) * raw_elem_size(combo);
+    const int pitch = (rb + 15) / 16 * 16;
+    return mb::stream_rows_smem(L, 16, cpb, stages, pitch) <= (size_t)dev_max_smem;
+  }
+
+  void add_stream_rows_kernel(int combo, int L, int64_t nbatch, AxisParams ap, int in_buf, int out_buf, int cpb,
+                              int stages, const TuneKey& key, bool vec_in, bool vec_out) {
+    Launch ln;
+    ln.key = key;
+    ln.radix = 16;
+    ln.fn = mb::stream_rows_kernel_fn(combo, ilog2(L));
+    ln.stream_rows = true;
+    const int esz = raw_elem_size(combo);
+    ap.cpb = cpb;
+    ap.nbatch = nbatch;
+    ap.nstages = stages;
+    ap.row_bytes = raw_row_elems(combo, L) * esz;
+    ap.row_pitch = (ap.row_bytes + 15) / 16 * 16;
+    ap.ntiles = (nbatch + cpb - 1) / cpb;
+    ap.lp = mb::tile_pitch(L, 16, cpb, 0);
+    ln.ch_static = pow2_align({int64_t(ap.row_bytes), ap.is0 * esz, ap.is1 * esz, ap.is2 * esz});
+    ln.smem = mb::stream_rows_smem(L, 16, cpb, stages, ap.row_pitch);
+    if (!ln.fn || ln.smem > (size_t)dev_max_smem) {
+      set_error(MINFFT_B200_EUNSUPPORTED, "no streamed row pass for combo %d, L=%d", combo, L);
+      ok = false;
+      return;
+    }
+    if (!a->host_only && !ensure_smem_attr(ln.fn, ln.smem)) {
+      ok = false;
+      return;
+    }
+    ln.block = unsigned(cpb * (L / 16));
+    int occ = 1;
+    if (!a->host_only) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ln.fn, (int)ln.block, ln.smem) != cudaSuccess ||
+          occ < 1) {
+        cudaGetLastError();
+        occ = 1;
+      }
+    }
+    ln.grid = unsigned(std::min<int64_t>(ap.ntiles, int64_t(sms) * occ));
+    ln.in_buf = in_buf;
+    ln.out_buf = out_buf;
+    ln.vec_in = vec_in;
+    ln.vec_out = vec_out;
+    ln.in_c = (combo == mb::K_CPLX || combo == mb::K_C2R || combo == mb::K_C2RQ);
+    ln.out_c = (combo == mb::K_CPLX || combo == mb::K_R2C || combo == mb::K_R2CQ);
+    ln.combo = combo;
+    ln.L = L;
+    ln.ap = ap;
+    {
+      static const char* names[] = {"cplx", "r2c", "c2r", "dct2", "dct3", "t4", "r2c+col4", "col4+c2r",
+                                    "t4pre+cplx", "cplx+t4post"};
+      const double Rb = sizeof(real), C = sizeof(cpx);
+      double per = 0;
+      switch (combo) {
+        case mb::K_CPLX: per = 2.0 * L * C; break;
+        case mb::K_R2C:
+        case mb::K_R2CQ: per = 2.0 * L * Rb + (L + 1) * C; break;
+        case mb::K_C2R:
+        case mb::K_C2RQ: per = (L + 1) * C + 2.0 * L * Rb; break;
+        default: per = 4.0 * L * Rb; break;
+      }
+      ln.bytes = per * double(nbatch);
+      char buf[160];
+      snprintf(buf, sizeof(buf), "stream_rows<%s,L=%d> batch=%lld", names[combo], L, (long long)nbatch);
+      ln.label = buf;
+    }
     prog->launches.push_back(ln);
   }
 
@@ -1760,6 +1862,18 @@ bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
     while (ch > 4 && (reinterpret_cast<uintptr_t>(ap.in) % ch) != 0) ch /= 2;
     ap.chunk = ch;
   }
+  if (ln.stream_rows) {
+    // one bulk copy per row where the rows start on 16-byte boundaries,
+    // else per-thread cp.async in the largest chunk the addresses allow
+    const uintptr_t base = reinterpret_cast<uintptr_t>(ap.in);
+    if ((base & 15) == 0 && ln.ch_static == 16)
+      ap.flags |= mb::F_STREAM_TMA;
+    int ch = ln.ch_static;
+    while (ch > 4 && (base % ch) != 0) ch /= 2;
+    ap.chunk = ch;
+    args[0] = &ap;
+    return enqueue(a, ln, args, ln.smem, "launch(stream rows)");
+  }
   if (ln.stream) {
     alignas(64) CUtensorMap map;
     memset(&map, 0, sizeof(map));
@@ -2330,9 +2444,19 @@ MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns,
                                                                  (ln.in_buf == BUF_Y && ln.out_buf == BUF_X)));
     if (alias_io && (ln.hbm_pass || (ln.is_line && ln.combo != mb::LK_UNIT)))
       fail("launch %zu (%s): runs in place but cannot", i, ln.label.c_str());
-    if (!ln.is_line && !ln.pipe && !ln.tc && !ln.stream && ln.grid > 0 &&
+    if (!ln.is_line && !ln.pipe && !ln.tc && !ln.stream && !ln.stream_rows && ln.grid > 0 &&
         int64_t(ln.grid) * ln.ap.cpb < ln.ap.nbatch)
       fail("launch %zu: grid does not cover the batch", i);
+    if (ln.stream_rows) {
+      const AxisParams& ap = ln.ap;
+      if (ap.colmode || ap.in_n != 1) fail("launch %zu (%s): streamed rows need contiguous rows", i, ln.label.c_str());
+      if (ap.ntiles * ap.cpb < ap.nbatch || ln.grid < 1 || int64_t(ln.grid) > ap.ntiles)
+        fail("launch %zu (%s): streamed row tiles do not cover the batch", i, ln.label.c_str());
+      if (ap.row_pitch < ap.row_bytes || ap.row_pitch % 16 || ap.nstages < 2 || ap.nstages > 8)
+        fail("launch %zu: streamed row stages", i);
+      if (ln.ch_static < 4 || ap.row_bytes % ln.ch_static)
+        fail("launch %zu: streamed row copy chunk %d", i, ln.ch_static);
+    }
     if (ln.stream) {
       const AxisParams& ap = ln.ap;
       const int W = mb::stream_cols();
@@ -2468,14 +2592,16 @@ MB_EXPORT int minfft_b200_autotune(minfft_aux* a, int op, int howmany, int reps)
     const Launch* base = nullptr;
     for (const Launch& ln : p0->launches)
       if (!ln.is_line && !ln.tc && !(ln.key < key) && !(key < ln.key)) base = &ln;
-    for (int cand = 0; cand < 6; ++cand) {
-      const int pipe = cand < 4 ? (cand & 1) : 2, radix = (cand & 2) ? 8 : 16;
+    for (int cand = 0; cand < 8; ++cand) {
+      const int pipe = cand < 4 ? (cand & 1) : (cand < 6 ? 2 : cand - 3), radix = (cand < 6 && (cand & 2)) ? 8 : 16;
       if (radix == 8 && key.L <= 8) continue;
       const int top = pipe == 2 ? 4 : probe.max_threads_cpb(key.L, radix);
       for (int cpb = pipe == 2 ? 2 : 1; cpb <= top; cpb = pipe == 2 ? cpb + 1 : 2 * cpb) {
-        if (Planner::four_rows(key.combo) && (pipe || cpb != 4)) continue;
+        if (Planner::four_rows(key.combo) && ((pipe != 3 && pipe != 4 && pipe) || cpb != 4)) continue;
         bool fits;
-        if (pipe == 2)
+        if (pipe == 3 || pipe == 4)
+          fits = base && probe.stream_rows_fits(key.combo, key.L, base->ap, cpb, pipe - 1);
+        else if (pipe == 2)
           fits = base && probe.stream_fits(key.combo, key.L, base->ap.nbatch, base->ap, radix, cpb);
         else if (pipe == 1)
           fits = probe.pipe_fits(key.combo, key.L, cpb, key.colmode, radix);
@@ -2556,7 +2682,7 @@ MB_EXPORT int minfft_b200_tune_load(const char* path) {
     long long nb, d0, in_n, out_k;
     if (sscanf(line, "%d %d %d %d %d %lld %lld %lld %lld %d %d %d", &k.combo, &k.L, &k.colmode, &k.hbm, &k.staged,
                &nb, &d0, &in_n, &out_k, &v.pipe, &v.cpb, &v.radix) == 12 &&
-        (v.radix == 8 || v.radix == 16) && v.pipe >= 0 && v.pipe <= 2) {
+        (v.radix == 8 || v.radix == 16) && v.pipe >= 0 && v.pipe <= 4) {
       k.nbatch = nb;
       k.d0 = d0;
       k.in_n = in_n;
@@ -2586,7 +2712,7 @@ MB_EXPORT int minfft_b200_tune_size(void) {
 // built afterwards use it.
 MB_EXPORT int minfft_b200_tune_set_default(int pipe, int cpb, int radix) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_default_override = TuneVal{pipe < 0 ? -1 : (pipe >= 2 ? 2 : (pipe ? 1 : 0)), cpb < 0 ? 0 : cpb, radix == 8 ? 8 : 16};
+  g_default_override = TuneVal{pipe < 0 ? -1 : std::min(pipe, 4), cpb < 0 ? 0 : cpb, radix == 8 ? 8 : 16};
   return MINFFT_B200_OK;
 }
 

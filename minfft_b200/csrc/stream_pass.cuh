@@ -263,3 +263,154 @@ __global__ void __launch_bounds__(stream_cols() * (L / R), 1)
 }
 
 }  // namespace mb
+
+namespace mb {
+
+// -------------------------------------------------------- streamed rows
+// The row-mode counterpart: persistent CTAs walk tiles of cpb transforms
+// whose input rows are contiguous; each row of a tile arrives in a stage of
+// shared memory by one bulk copy (cp.async.bulk, no tensor map) or, where
+// the row's bytes or addresses break the 16-byte rules, by per-thread
+// cp.async, counted by the stage's mbarrier.  The kind's own load stage
+// (LoadR2C, LoadDCT2, LoadT4, LoadC2R, LoadDCT3, LoadC2RQ, LoadCplx) then
+// reads the row from the stage instead of global memory -- the same index
+// arithmetic on a shared-memory base -- and the stage is refilled with the
+// tile S steps ahead right away, so the next tiles' rows stream in while this
+// one is transformed in the padded exchange tile and stored by the kind's
+// store stage.  Waits are bounded as in the column form.
+__host__ __device__ inline size_t stream_rows_offsets_bytes(int cpb) {
+  return 16 * ((2 * size_t(cpb) * sizeof(int64_t) + 15) / 16);
+}
+__host__ __device__ inline size_t stream_rows_tile_bytes(int L, int R, int cpb) {
+  return (size_t(cpb) * tile_pitch(L, R, cpb, 0) * sizeof(cpx) + 127) / 128 * 128;
+}
+__host__ __device__ inline size_t stream_rows_smem(int L, int R, int cpb, int stages, int row_pitch) {
+  return 128 + (stream_rows_offsets_bytes(cpb) + 127) / 128 * 128 + stream_rows_tile_bytes(L, R, cpb) +
+         size_t(stages) * cpb * row_pitch;
+}
+
+template <int L, int R, class LoadOp, class StoreOp>
+__global__ void __launch_bounds__(512, 1) stream_rows_kernel(const AxisParams p) {
+  constexpr int TPT = L / R;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);
+  int* bad = reinterpret_cast<int*>(smem + 64);
+  const int cpb = p.cpb, S = p.nstages;
+  int64_t* offs = reinterpret_cast<int64_t*>(smem + 128);
+  unsigned char* tile_raw = smem + 128 + (stream_rows_offsets_bytes(cpb) + 127) / 128 * 128;
+  unsigned char* stages = tile_raw + stream_rows_tile_bytes(L, R, cpb);
+  const int stage_bytes = cpb * p.row_pitch;
+  const int tid = threadIdx.x;
+  const bool bulk = (p.flags & F_STREAM_TMA) != 0;
+  const uint32_t mbar0 = static_cast<uint32_t>(__cvta_generic_to_shared(mbar));
+  const uint32_t st0 = static_cast<uint32_t>(__cvta_generic_to_shared(stages));
+  const int64_t ntiles = p.ntiles;
+  constexpr int esz = LoadOp::kComplexIn ? int(sizeof(cpx)) : int(sizeof(real));
+
+  pdl_release();
+  pdl_wait();
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) smbar_init(mbar0 + 8 * s, bulk ? 1 : int(blockDim.x));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *bad = 0;
+  }
+  __syncthreads();
+
+  auto issue = [&](int64_t t, int s) {
+    if (t >= ntiles) return;
+    const int64_t b0t = t * cpb;
+    const int nv = int(p.nbatch - b0t < cpb ? p.nbatch - b0t : cpb);
+    const uint32_t mb = mbar0 + 8 * s;
+    const uint32_t dst = st0 + uint32_t(s) * uint32_t(stage_bytes);
+    const char* in = static_cast<const char*>(p.in);
+    if (bulk) {
+      if (tid == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(nv * p.row_bytes)
+                     : "memory");
+        for (int c = 0; c < nv; ++c) {
+          int64_t b0, oi, oo;
+          batch_offsets(p, b0t + c, b0, oi, oo);
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                  dst + uint32_t(c * p.row_pitch)),
+              "l"(in + oi * esz), "r"(p.row_bytes), "r"(mb)
+              : "memory");
+        }
+      }
+    } else {
+      const int ch = p.chunk;
+      const int cpr = p.row_bytes / ch;
+      for (int e = tid; e < nv * cpr; e += blockDim.x) {
+        const int c = e / cpr, k = e - c * cpr;
+        int64_t b0, oi, oo;
+        batch_offsets(p, b0t + c, b0, oi, oo);
+        const char* g = in + oi * esz + int64_t(k) * ch;
+        const uint32_t d = dst + uint32_t(c * p.row_pitch + k * ch);
+        if (ch == 16)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g) : "memory");
+        else if (ch == 8)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(g) : "memory");
+        else
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(g) : "memory");
+      }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(mb) : "memory");
+    }
+  };
+
+  for (int s = 0; s < S; ++s) issue(blockIdx.x + int64_t(s) * gridDim.x, s);
+
+  Tile tl{reinterpret_cast<cpx*>(tile_raw), p.lp};
+  int it = 0;
+  bool ok = true;
+  int64_t t = blockIdx.x;
+  for (; t < ntiles; t += gridDim.x, ++it) {
+    const int s = it % S;
+    if (!smbar_wait(mbar0 + 8 * s, uint32_t(it / S) & 1u, kStreamSpinLimit)) atomicExch(bad, 1);
+    __syncthreads();
+    if (*bad) {
+      ok = false;
+      break;
+    }
+    const int64_t b0t = t * cpb;
+    const int nv = int(p.nbatch - b0t < cpb ? p.nbatch - b0t : cpb);
+    for (int c = tid; c < cpb; c += blockDim.x) {
+      int64_t b0, oi, oo;
+      batch_offsets(p, b0t + c < p.nbatch ? b0t + c : 0, b0, oi, oo);
+      offs[c] = oi;
+      offs[cpb + c] = oo;
+    }
+    __syncthreads();
+    TileOffsets to{offs, offs + cpb, nv};
+    Ctx x;
+    x.j = tid % TPT;
+    x.c = tid / TPT;
+    x.b = b0t + x.c;
+    x.active = x.c < nv;
+    x.b0 = x.b % p.d0;
+    x.oin = int64_t(x.c) * (p.row_pitch / esz);
+    x.oout = offs[cpb + x.c];
+    // the kind's load stage, on the rows in the stage
+    AxisParams pl = p;
+    pl.in = stages + size_t(s) * stage_bytes;
+    pl.in_n = 1;
+    pl.is0 = p.row_pitch / esz;
+    pl.flags |= F_VEC;
+    cpx v[R];
+    LoadOp::template run<L, R>(pl, x, tl, v);
+    __syncthreads();  // every read of the stage is done: refill it
+    if (bulk && tid == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    issue(t + int64_t(S) * gridDim.x, s);
+    run_passes<L, R, 1>(v, x.j, x.c, tl, p.tw);
+    StoreOp::template run<L, R>(p, x, tl, to, v);
+    __syncthreads();
+  }
+  if (!ok) {
+    if (tid == 0 && p.status) atomicExch(p.status, 1);
+    for (int k = 0; k < S; ++k, ++it, t += gridDim.x) {
+      if (t >= ntiles) break;
+      smbar_wait(mbar0 + 8 * (it % S), uint32_t(it / S) & 1u, kStreamSpinLimit);
+    }
+  }
+}
+
+}  // namespace mb

@@ -83,6 +83,7 @@ def test_tc_wait_timeout_is_reported_and_the_plan_recovers():
         try:
             plan("dft", xt.data_ptr(), y.data_ptr())
             assert L.minfft_b200_device_status(plan.aux) == 5  # MINFFT_B200_ETIMEOUT
+            assert eng.last_error() == 5  # also the thread's last error (read and cleared here)
         finally:
             L.minfft_b200_test_tc_withhold(0)
         assert L.minfft_b200_device_status(plan.aux) == 0  # the record was cleared

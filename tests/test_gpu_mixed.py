@@ -126,3 +126,26 @@ def test_mixed_plan_rejects_bad_jobs(single):
         with pytest.raises(minfft_b200.MinfftError) as e:
             eng.mixed_plan(jobs)
         assert e.value.code == 1
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+def test_mixed_cluster_form_every_long_kind(single, monkeypatch):
+    """The cluster form of the long items (2^14 .. 2^16 complex points on
+    eight CTAs in distributed shared memory, MINFFT_B200_MIXED_CLUSTER=1):
+    every kind and long length, mixed with short items, against the oracle."""
+    monkeypatch.setenv("MINFFT_B200_MIXED_CLUSTER", "1")
+    rng = np.random.default_rng(17)
+    specs = []
+    for op in minfft_b200.OPS:
+        lens = (14, 15, 16) if op in ("dft", "invdft") else (15, 16, 17)
+        specs += [(op, 1 << lg) for lg in lens]
+    specs += [("dct2", 256)] * 8 + [("dft", 64)] * 8 + [("dst4", 1 << 12)] * 4
+    eng = minfft_b200.engine(single)
+    pool, jobs, host = make_batch(single, specs, rng)
+    h = eng.mixed_plan(jobs)
+    try:
+        eng.mixed_execute(h)
+        torch.cuda.synchronize()
+        check_batch(single, pool, host)
+    finally:
+        eng.mixed_free(h)

@@ -104,3 +104,32 @@ def test_fused_type4_chain_matches_oracle(single):
     x = make_input("dst4", dims, rng, single)
     err = rel_l2(gpu_apply("dst4", x, dims, single, inplace=True), expected("dst4", x, dims))
     assert err <= tolerance(single, dims)
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+@pytest.mark.parametrize("form,cpb", [(3, 0), (3, 1), (4, 2), (4, 8)])
+def test_streamed_rows_match_oracle(single, form, cpb):
+    """The streamed row pass (bulk row copies into mbarrier stages, each
+    kind's load stage reading the stage): forced as the default form (3: two
+    stages, 4: three) for every transform kind, on rows of 2-D arrays (the
+    split-column kinds of the 2048-row real DFT included), batches with a
+    partial last tile, rows of odd byte length (the inverse real DFT's
+    L+1 complex values in single precision: cp.async), in place."""
+    eng = minfft_b200.engine(single)
+    rng = np.random.default_rng(64)
+    try:
+        eng.tune_clear()
+        eng.tune_set_default(form, cpb, 16)
+        assert any("stream_rows" in lab for lab in labels(eng, "dct2", (64, 512)))
+        for dims in [(64, 512), (5, 2048), (2048, 256), (2048, 2048), (3, 64, 128)]:
+            for op in minfft_b200.OPS:
+                x = make_input(op, dims, rng, single)
+                err = rel_l2(gpu_apply(op, x, dims, single), expected(op, x, dims))
+                assert err <= tolerance(single, dims), (op, dims, form, cpb, err)
+        dims = (32, 1024)
+        for op in ("realdft", "dct3"):
+            x = make_input(op, dims, rng, single)
+            err = rel_l2(gpu_apply(op, x, dims, single, inplace=True), expected(op, x, dims))
+            assert err <= tolerance(single, dims), (op, "in place", err)
+    finally:
+        eng.tune_set_default(-1, 0, 16)
