@@ -91,6 +91,7 @@ struct AxisParams {
 };
 
 enum : int {
+  F_SRC_SMEM = 1 << 9,  // the input pointer is a shared-memory stage (generic loads, no ld.global)
   F_CONJ_IN = 1,      // conjugate the input (inverse DFT = conj . DFT . conj)
   F_CONJ_OUT = 2,     // conjugate the output
   F_DST = 4,          // sine variant of a real symmetric transform
@@ -255,6 +256,14 @@ __device__ __forceinline__ void run_passes(cpx (&v)[R], int j, int c, const Tile
   }
 }
 
+// A streaming (evict-first) load from global memory, or a plain load where
+// the kernel reads its input from a shared-memory stage (F_SRC_SMEM): the
+// streaming form is a global-only instruction.
+template <typename T>
+__device__ __forceinline__ T src_ld(const T* q, bool smem) {
+  return smem ? *q : __ldcs(q);
+}
+
 // ------------------------------------------------------------- row staging
 // In row mode a transform's real row (N = 2L contiguous reals) is moved
 // between global memory and the transform's tile slot in shared memory by its
@@ -269,7 +278,7 @@ __device__ __forceinline__ void run_passes(cpx (&v)[R], int j, int c, const Tile
 __device__ __forceinline__ real* tile_row(const Tile& t, int c) { return reinterpret_cast<real*>(t.s + c * t.lp); }
 
 template <int L, int R>
-__device__ __forceinline__ void row_g2s(real* sr, const real* g, int j) {
+__device__ __forceinline__ void row_g2s(real* sr, const real* g, int j, bool smem = false) {
   constexpr int TPT = L / R;
   constexpr int NV = 2 * L * int(sizeof(real)) / 16;  // 16-byte vectors in the row
   static_assert(NV % TPT == 0, "whole vectors per thread");
@@ -278,13 +287,13 @@ __device__ __forceinline__ void row_g2s(real* sr, const real* g, int j) {
     uint4* sv = reinterpret_cast<uint4*>(sr) + j;
     uint4 r[NV / TPT];
 #pragma unroll
-    for (int i = 0; i < NV / TPT; ++i) r[i] = __ldcs(gv + i * TPT);
+    for (int i = 0; i < NV / TPT; ++i) r[i] = src_ld(gv + i * TPT, smem);
 #pragma unroll
     for (int i = 0; i < NV / TPT; ++i) sv[i * TPT] = r[i];
   } else {
     real r[2 * R];
 #pragma unroll
-    for (int i = 0; i < 2 * R; ++i) r[i] = __ldcs(g + j + i * TPT);
+    for (int i = 0; i < 2 * R; ++i) r[i] = src_ld(g + j + i * TPT, smem);
 #pragma unroll
     for (int i = 0; i < 2 * R; ++i) sr[j + i * TPT] = r[i];
   }
@@ -317,11 +326,11 @@ __device__ __forceinline__ void row_s2g(real* g, const real* sr, int j) {
 // issued before any store; a warp's load covers cpb adjacent columns of a
 // few rows.
 template <int L, int R>
-__device__ __forceinline__ void col_g2s(real* sr, const real* g, int64_t s, int j) {
+__device__ __forceinline__ void col_g2s(real* sr, const real* g, int64_t s, int j, bool smem = false) {
   constexpr int TPT = L / R;
   real r[2 * R];
 #pragma unroll
-  for (int m = 0; m < 2 * R; ++m) r[m] = __ldcs(g + int64_t(j + m * TPT) * s);
+  for (int m = 0; m < 2 * R; ++m) r[m] = src_ld(g + int64_t(j + m * TPT) * s, smem);
 #pragma unroll
   for (int m = 0; m < 2 * R; ++m) sr[j + m * TPT] = r[m];
 }
@@ -389,12 +398,12 @@ struct LoadCplx {
     } else if (p.in_n == 1) {  // contiguous: compile-time offsets
       const cpx* q = in + x.j;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = __ldcs(q + r * TPT);
+      for (int r = 0; r < R; ++r) v[r] = src_ld(q + r * TPT, (p.flags & F_SRC_SMEM) != 0);
     } else {
       const cpx* q = in + x.j * p.in_n;
       const int64_t st = int64_t(TPT) * p.in_n;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = __ldcs(q + r * st);
+      for (int r = 0; r < R; ++r) v[r] = src_ld(q + r * st, (p.flags & F_SRC_SMEM) != 0);
     }
     if (p.flags & F_CONJ_IN) {
 #pragma unroll
@@ -419,7 +428,7 @@ struct LoadR2C {
     } else if (p.flags & F_VEC) {
       const cpx* q = reinterpret_cast<const cpx*>(in) + x.j;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = __ldcs(q + r * TPT);
+      for (int r = 0; r < R; ++r) v[r] = src_ld(q + r * TPT, (p.flags & F_SRC_SMEM) != 0);
     } else {
       const real* q = in + 2 * x.j;
 #pragma unroll
@@ -676,9 +685,9 @@ struct LoadDCT3 {
         real* sr = tile_row(t, x.c);
         if (x.active) {
           if (p.colmode)
-            col_g2s<L, R>(sr, in, p.in_n, x.j);
+            col_g2s<L, R>(sr, in, p.in_n, x.j, (p.flags & F_SRC_SMEM) != 0);
           else
-            row_g2s<L, R>(sr, in, x.j);
+            row_g2s<L, R>(sr, in, x.j, (p.flags & F_SRC_SMEM) != 0);
         }
         __syncthreads();
         constexpr int NP = R / 2 + 1;

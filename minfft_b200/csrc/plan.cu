@@ -619,14 +619,26 @@ struct Planner {
     ap.ntiles = ap.gpb * ap.d1 * ln.st_d2;
     ap.lp = 0;
     ln.block = unsigned(mb::kTcStreamThreads);
+    // resident CTAs per SM, counted here from registers, shared memory,
+    // threads and the 128 tensor-memory columns a CTA allocates (the
+    // occupancy calculator reports one CTA per SM for kernels that allocate
+    // tensor memory)
     int occ = 1;
     if (!a->host_only) {
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ln.fn, (int)ln.block, ln.smem) != cudaSuccess ||
-          occ < 1) {
+      cudaFuncAttributes fa;
+      int dev = 0, smem_sm = 0, regs_sm = 0;
+      if (cudaFuncGetAttributes(&fa, ln.fn) == cudaSuccess && cudaGetDevice(&dev) == cudaSuccess &&
+          cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+          cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) == cudaSuccess) {
+        const int warps = int(ln.block + 31) / 32;
+        const int regs_cta = warps * ((fa.numRegs * 32 + 255) / 256 * 256);
+        const size_t smem_cta = ln.smem + fa.sharedSizeBytes + 1024;  // + the per-CTA reservation
+        occ = std::min({regs_sm / std::max(regs_cta, 1), int(size_t(smem_sm) / smem_cta), 2048 / int(ln.block),
+                        512 / 128});
+        occ = std::max(occ, 1);
+      } else {
         cudaGetLastError();
-        occ = 1;
       }
-      occ = std::min(occ, 512 / 128);  // tensor memory: 128 columns per CTA
     }
     ln.grid = unsigned(std::min<int64_t>(ap.ntiles, int64_t(sms) * occ));
     ln.in_buf = in_buf;

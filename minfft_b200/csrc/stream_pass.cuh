@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(512, 1) stream_rows_kernel(const AxisParams p)
     pl.in = stages + size_t(s) * stage_bytes;
     pl.in_n = 1;
     pl.is0 = p.row_pitch / esz;
-    pl.flags |= F_VEC;
+    pl.flags |= F_VEC | F_SRC_SMEM;
     cpx v[R];
     LoadOp::template run<L, R>(pl, x, tl, v);
     __syncthreads();  // every read of the stage is done: refill it
