@@ -38,6 +38,7 @@
 #include "kernel_registry.h"
 #include "pipe_pass.cuh"
 #include "stream_pass.cuh"
+#include "dct_split.h"
 #include "line_kernels.h"
 #include "tc_pass.h"
 #include "minfft.h"
@@ -257,6 +258,9 @@ struct Launch {
   bool stream = false;   // persistent TMA-fed column pass (stream_pass.cuh)
   bool stream_rows = false;  // persistent bulk-copy-fed row pass (stream_pass.cuh)
   int tcs = 0;           // tensor-core pass in streamed form: 1 column tiles, 2 row tiles
+  int dctq = -1;         // split-column DCT pass (dct_split.cu): mb::dctq_kernel's `which`, else -1
+  mb::DctqParams dq{};   // its parameters (in, out, mid resolved at launch)
+  int mid_buf = -1;      // its intermediate buffer
   int64_t st_d2 = 1;     // streamed pass: outermost batch extent of its tensor copies
   bool tc = false;       // tensor-core split-precision pass (tc_pass.cu)
   mb::TcParams tcp{};    // its B operands and status word
@@ -1257,6 +1261,73 @@ struct Planner {
 
   // Forward: rows X -> block layout in `mid` (row j of block q at (q*Q + j)*K),
   // then length-Q column DFTs mid -> Y (output p of block q at row q + 4p).
+  // Split column DFT of the 2-D DCT-2/DST-2 and DCT-3/DST-3 (Nr rows of N
+  // reals): Nr = 8Q with Q = 64 .. 512, N/2 = 64 .. 1024, from the same row
+  // count as the split 2-D real DFT (MINFFT_B200_SPLIT2D).
+  int dctq_cols(int64_t Q) const {
+    int W = int(128 / sizeof(cpx));
+    while (W > 1 && 2 * W * (Q / 16) > 512) W /= 2;
+    return W;
+  }
+  bool split_dct(int64_t Nr, int64_t N) const {
+    if (!split_2d(Nr, N) || Nr % 8 != 0) return false;
+    const int64_t Q = Nr / 8, L = N / 2;
+    if (!mb::dctq_kernel(0, ilog2(L)) || !mb::dctq_kernel(1, ilog2(Q)) || !is_pow2(Q)) return false;
+    const int W = dctq_cols(Q);
+    if (N % W != 0) return false;
+    return mb::dctq_row_smem(int(L)) <= (size_t)dev_max_smem && mb::dctq_col_smem(int(Q), W) <= (size_t)dev_max_smem;
+  }
+
+  void add_dctq(int which, int64_t H, int64_t Nr, int64_t N, int flags, int in_buf, int out_buf, int mid) {
+    const int64_t Q = Nr / 8, L = N / 2, Lc = Nr / 2;
+    const bool row = (which == 0 || which == 3);
+    Launch ln;
+    ln.dctq = which;
+    ln.fn = mb::dctq_kernel(which, ilog2(row ? L : Q));
+    ln.radix = 16;
+    mb::DctqParams& d = ln.dq;
+    d.H = H;
+    d.Nr = Nr;
+    d.N = N;
+    d.Q = Q;
+    d.flags = flags;
+    d.W = dctq_cols(Q);
+    d.lp = row ? mb::tile_pitch(int(L), 16, 8, 0) : mb::tile_pitch(int(Q), 16, 2 * d.W, 1);
+    d.tw_row = tab(TB_TW, L);
+    d.rft_row = tab(TB_RFT, N);
+    d.t23_row = tab(TB_T23, N);
+    d.tw_c = tab(TB_TW, Lc);
+    d.tw_q = tab(TB_TW, Q);
+    d.rft_c = tab(TB_RFT, Nr);
+    d.t23_c = tab(TB_T23, Nr);
+    ln.smem = row ? mb::dctq_row_smem(int(L)) : mb::dctq_col_smem(int(Q), d.W);
+    if (!ln.fn || ln.smem > (size_t)dev_max_smem) {
+      set_error(MINFFT_B200_EUNSUPPORTED, "no split DCT pass for %lld x %lld", (long long)Nr, (long long)N);
+      ok = false;
+      return;
+    }
+    if (!a->host_only && !ensure_smem_attr(ln.fn, ln.smem)) {
+      ok = false;
+      return;
+    }
+    ln.block = unsigned(row ? 8 * (L / 16) : 2 * d.W * (Q / 16));
+    ln.grid = unsigned(row ? H * Q : H * 2 * (N / d.W));
+    ln.in_buf = in_buf;
+    ln.out_buf = out_buf;
+    ln.mid_buf = mid;
+    ln.in_c = (which == 1 || which == 3);
+    ln.out_c = false;
+    ln.L = int(row ? L : Q);
+    const double R = sizeof(real), C = sizeof(cpx);
+    ln.bytes = double(H) * Nr * N * R + double(H) * Lc * N * C;  // the real array and the blocks
+    static const char* names[] = {"dct2 rows+col4", "col4 dct2 cols", "dct3 cols col4", "col4+dct3 rows"};
+    char buf[160];
+    snprintf(buf, sizeof(buf), "dct_split<%s,%s=%lld> %lldx%lld", names[which], row ? "L" : "Q",
+             (long long)(row ? L : Q), (long long)Nr, (long long)N);
+    ln.label = buf;
+    prog->launches.push_back(ln);
+  }
+
   // Row pitch of the intermediate of a split 2-D real DFT: K complex values
   // rounded up to whole 16-byte units, so that its columns can be fetched
   // with tensor copies (the extra column is never read).
@@ -1667,6 +1738,19 @@ bool build_program(minfft_aux* a, int op, int howmany, bool alias, Program* prog
       if (op == MINFFT_B200_DCT2 || op == MINFFT_B200_DST2) combo = mb::K_DCT2;
       if (op == MINFFT_B200_DCT3 || op == MINFFT_B200_DST3) combo = mb::K_DCT3;
       if (op == MINFFT_B200_DST2 || op == MINFFT_B200_DST3 || op == MINFFT_B200_DST4) fl = mb::F_DST;
+      if (nd == 3 && combo != mb::K_T4 && pl.split_dct(D[1], D[2])) {
+        // the 2-D split column DFT: blocks of the column DFT in T1
+        const size_t blocks = size_t(D[0] * D[1] * D[2]) * sizeof(real);
+        pl.need(BUF_T1, blocks);
+        if (combo == mb::K_DCT2) {
+          pl.add_dctq(0, D[0], D[1], D[2], fl, BUF_X, BUF_T1, BUF_T1);
+          pl.add_dctq(1, D[0], D[1], D[2], fl, BUF_T1, BUF_Y, BUF_T1);
+        } else {
+          pl.add_dctq(2, D[0], D[1], D[2], fl, BUF_X, BUF_T1, BUF_T1);
+          pl.add_dctq(3, D[0], D[1], D[2], fl, BUF_T1, BUF_Y, BUF_T1);
+        }
+        break;
+      }
       int cur = BUF_X;
       for (size_t ax = nd - 1; ax >= 1; --ax) {
         AxisStep s{};
@@ -1873,6 +1957,22 @@ bool launch_one(minfft_aux* a, const Launch& ln, void* const* bufs) {
     int ch = ln.ch_static;
     while (ch > 4 && (reinterpret_cast<uintptr_t>(ap.in) % ch) != 0) ch /= 2;
     ap.chunk = ch;
+  }
+  if (ln.dctq >= 0) {
+    mb::DctqParams d = ln.dq;
+    d.in = bufs[ln.in_buf];
+    d.out = bufs[ln.out_buf];
+    d.mid = static_cast<cpx*>(bufs[ln.mid_buf]);
+    void* dargs[1] = {&d};
+    return enqueue(a, ln, dargs, ln.smem, "launch(dct split)");
+  }
+  if (ln.dctq >= 0) {
+    mb::DctqParams d = ln.dq;
+    d.in = bufs[ln.in_buf];
+    d.out = bufs[ln.out_buf];
+    d.mid = static_cast<cpx*>(bufs[ln.mid_buf]);
+    void* dargs[1] = {&d};
+    return enqueue(a, ln, dargs, ln.smem, "launch(dct split)");
   }
   if (ln.stream_rows) {
     // one bulk copy per row where the rows start on 16-byte boundaries,
@@ -2334,6 +2434,12 @@ void axis_batch_max(const AxisParams& ap, int64_t& oi, int64_t& oo) {
 
 Extent launch_extent(const Launch& ln) {
   Extent e{0, 0};
+  if (ln.dctq >= 0) {  // the whole real array and the whole block array
+    const int64_t reals = ln.dq.H * ln.dq.Nr * ln.dq.N, blocks = ln.dq.H * (ln.dq.Nr / 2) * ln.dq.N;
+    e.in_max = (ln.in_c ? blocks : reals) - 1;
+    e.out_max = (ln.in_c ? reals : blocks) - 1;
+    return e;
+  }
   if (!ln.is_line) {
     const AxisParams& ap = ln.ap;
     const int64_t L = ln.L;
@@ -2448,7 +2554,7 @@ MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns,
            (long long)((e.out_max + 1) * oe), ln.out_buf, cap[ln.out_buf]);
     if (ln.block < 1 || ln.block > 1024 || ln.grid < 1) fail("launch %zu: bad shape %u x %u", i, ln.grid, ln.block);
     if (!ln.is_line && ln.block > 512) fail("launch %zu: block %u above launch bounds", i, ln.block);
-    if (!ln.is_line && !ln.stream && !ln.tcs &&
+    if (!ln.is_line && !ln.stream && !ln.tcs && ln.dctq < 0 &&
         ln.block != unsigned(ln.ap.cpb * (ln.L / std::min(ln.radix, std::max(ln.L, 1)))))
       fail("launch %zu: block %u is not cpb x L/R", i, ln.block);
     if (ln.smem > size_t(di.max_smem)) fail("launch %zu: %zu bytes of shared memory", i, ln.smem);
@@ -2456,7 +2562,7 @@ MB_EXPORT int minfft_b200_plan_selfcheck_precision(int op, int d, const int* Ns,
                                                                  (ln.in_buf == BUF_Y && ln.out_buf == BUF_X)));
     if (alias_io && (ln.hbm_pass || (ln.is_line && ln.combo != mb::LK_UNIT)))
       fail("launch %zu (%s): runs in place but cannot", i, ln.label.c_str());
-    if (!ln.is_line && !ln.pipe && !ln.tc && !ln.stream && !ln.stream_rows && ln.grid > 0 &&
+    if (!ln.is_line && !ln.pipe && !ln.tc && !ln.stream && !ln.stream_rows && ln.dctq < 0 && ln.grid > 0 &&
         int64_t(ln.grid) * ln.ap.cpb < ln.ap.nbatch)
       fail("launch %zu: grid does not cover the batch", i);
     if (ln.stream_rows) {
@@ -2581,7 +2687,7 @@ MB_EXPORT int minfft_b200_autotune(minfft_aux* a, int op, int howmany, int reps)
   if (!p0) return g_err ? g_err : MINFFT_B200_ECUDA;
   std::vector<TuneKey> keys;
   for (const Launch& ln : p0->launches)
-    if (!ln.is_line && !ln.tc) keys.push_back(ln.key);
+    if (!ln.is_line && !ln.tc && ln.dctq < 0) keys.push_back(ln.key);
   const size_t in_b = size_t(io_bytes(a, op, false)) * howmany, out_b = size_t(io_bytes(a, op, true)) * howmany;
   void *x = nullptr, *y = nullptr;
   if (!cuda_ok(cudaMalloc(&x, in_b), "cudaMalloc(autotune)")) return g_err;
@@ -2603,7 +2709,7 @@ MB_EXPORT int minfft_b200_autotune(minfft_aux* a, int op, int howmany, int reps)
     // the launch's own parameters (for the streamed form's applicability)
     const Launch* base = nullptr;
     for (const Launch& ln : p0->launches)
-      if (!ln.is_line && !ln.tc && !(ln.key < key) && !(key < ln.key)) base = &ln;
+      if (!ln.is_line && !ln.tc && ln.dctq < 0 && !(ln.key < key) && !(key < ln.key)) base = &ln;
     for (int cand = 0; cand < 8; ++cand) {
       const int pipe = cand < 4 ? (cand & 1) : (cand < 6 ? 2 : cand - 3), radix = (cand < 6 && (cand & 2)) ? 8 : 16;
       if (radix == 8 && key.L <= 8) continue;
