@@ -189,9 +189,17 @@ __global__ void __launch_bounds__(512, 1) dctq_col_fwd(const DctqParams q) {
     int64_t k;
     cpx za, zb;
     if (P == 1) {
+      // the pair (k, Lc-k) with k = 1 + 4p in block 1 and Lc-k in block 3,
+      // taken from its smaller member (the root table holds w_Nr^k for k < Lc/2)
       k = 1 + 4 * int64_t(pi);
       za = t.s[t.idx(cc, pi)];
       zb = t.s[t.idx(W + cc, QL - 1 - pi)];
+      if (2 * k > Lc) {
+        const cpx tmp = za;
+        za = zb;
+        zb = tmp;
+        k = Lc - k;
+      }
     } else if (pi <= QL / 2) {
       k = 4 * int64_t(pi);
       za = t.s[t.idx(cc, pi)];
@@ -243,12 +251,18 @@ __global__ void __launch_bounds__(512, 1) dctq_col_inv(const DctqParams q) {
     const int cc = e % W, pi = e / W;
     auto rd = [&](int i) { return in[int64_t(i) * N + cc]; };
     auto z = [&](int64_t k) { return LoadDCT3::zval_r(rd, int(k), int(Lc), dst, q.t23_c); };
-    if (P == 1) {  // k = 1 + 4p, partner 3 + 4(Q-1-p)
+    if (P == 1) {  // k = 1 + 4p, partner 3 + 4(Q-1-p); packed from the smaller member
       const int64_t k = 1 + 4 * int64_t(pi);
       cpx ta, tb;
-      pack_pair(z(k), z(Lc - k), ldg(q.rft_c + k), ta, tb);
-      t.s[t.idx(cc, pi)] = cconj(ta);
-      t.s[t.idx(W + cc, QL - 1 - pi)] = cconj(tb);
+      if (2 * k < Lc) {
+        pack_pair(z(k), z(Lc - k), ldg(q.rft_c + k), ta, tb);
+        t.s[t.idx(cc, pi)] = cconj(ta);
+        t.s[t.idx(W + cc, QL - 1 - pi)] = cconj(tb);
+      } else {
+        pack_pair(z(Lc - k), z(k), ldg(q.rft_c + (Lc - k)), ta, tb);
+        t.s[t.idx(W + cc, QL - 1 - pi)] = cconj(ta);
+        t.s[t.idx(cc, pi)] = cconj(tb);
+      }
     } else if (pi <= QL / 2) {  // k = 4p, partner 4(Q-p) (k = 0 pairs with Lc)
       const int64_t k = 4 * int64_t(pi);
       const cpx z0 = z(k);

@@ -1263,14 +1263,17 @@ struct Planner {
   // then length-Q column DFTs mid -> Y (output p of block q at row q + 4p).
   // Split column DFT of the 2-D DCT-2/DST-2 and DCT-3/DST-3 (Nr rows of N
   // reals): Nr = 8Q with Q = 64 .. 512, N/2 = 64 .. 1024, from the same row
-  // count as the split 2-D real DFT (MINFFT_B200_SPLIT2D).
+  // count as the split 2-D real DFT (MINFFT_B200_SPLIT2D), when enabled.
   int dctq_cols(int64_t Q) const {
     int W = int(128 / sizeof(cpx));
     while (W > 1 && 2 * W * (Q / 16) > 512) W /= 2;
     return W;
   }
   bool split_dct(int64_t Nr, int64_t N) const {
-    if (!split_2d(Nr, N) || Nr % 8 != 0) return false;
+    // opt-in (MINFFT_B200_SPLITDCT=1): measured slower than the one-tile row
+    // and column passes on 2048 x 2048 in both precisions
+    const char* env = getenv("MINFFT_B200_SPLITDCT");  // read at each planning
+    if (!(env && env[0] == '1') || !split_2d(Nr, N) || Nr % 8 != 0) return false;
     const int64_t Q = Nr / 8, L = N / 2;
     if (!mb::dctq_kernel(0, ilog2(L)) || !mb::dctq_kernel(1, ilog2(Q)) || !is_pow2(Q)) return false;
     const int W = dctq_cols(Q);

@@ -15,6 +15,12 @@ from test_gpu_parity import expected, gpu_apply, make_input
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(autouse=True)
+def split_on(monkeypatch):
+    """The split form is opt-in; plans made in these tests take it."""
+    monkeypatch.setenv("MINFFT_B200_SPLITDCT", "1")
+
 KINDS = ("dct2", "dst2", "dct3", "dst3")
 SHAPES = [(1024, 128), (2048, 2048), (4096, 256), (1024, 2048)]
 
