@@ -559,7 +559,8 @@ struct TcsLayout {
   static constexpr int NT = FMT == TC_F16 ? 2 : 3;
   static constexpr int bar_bytes = 128;                  // mbarriers, TMEM slot, flag
   static constexpr int b_off = bar_bytes;                // B operands: NT x 2 KB
-  static constexpr int a_off = b_off + NT * kBBytes;     // A operands: 2 groups x NT x 8 KB
+  static constexpr int tw_off = b_off + NT * kBBytes;    // w_256^m, m < 256 (2 KB)
+  static constexpr int a_off = tw_off + kL * 8;          // A operands: 2 groups x NT x 8 KB
   static constexpr int st_off = a_off + 2 * NT * kOpBytes;
   static constexpr int tmem_cols = 128;                  // 2 groups x (leading, correction) x 32
 };
@@ -673,6 +674,7 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + 80);
   int* bad = reinterpret_cast<int*>(sm + 84);
   unsigned char* bop = sm + Lay::b_off;
+  cpx* tws = reinterpret_cast<cpx*>(sm + Lay::tw_off);
   unsigned char* aop = sm + Lay::a_off;
   unsigned char* stages = sm + Lay::st_off;
   const int S = p.cpb;
@@ -709,6 +711,7 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
     const uint4* src = reinterpret_cast<const uint4*>(q.bmat);
     uint4* dst = reinterpret_cast<uint4*>(bop);
     for (int i = tid; i < NT * kBBytes / 16; i += kTcsNT) dst[i] = src[i];
+    tws[tid] = ldg(p.tw + tid);  // the twiddles between the stages, read from shared memory
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -843,7 +846,7 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
     // unscale and twiddle: y1[k1][n2] * w_256^(n2 k1), n2 = d; into the stage
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) {
-      const cpx w = ldg(p.tw + d * k1);
+      const cpx w = tws[d * k1];
       const cpx y = cmul(cmk(re[k1] * inv, im[k1] * inv), w);
       const int idx = ROWS ? c * kL + 16 * k1 + (d ^ k1) : (16 * k1 + d) * W + c;
       tile[idx] = y;
