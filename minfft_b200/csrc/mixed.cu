@@ -14,13 +14,14 @@
 // atomic counter until the list is exhausted.  Short items run the same
 // load -> Stockham passes -> store code as the axis passes, with each
 // transform's own input and output pointers.  Long items (2^14 .. 2^16
-// complex points) run on clusters of eight CTAs entirely in distributed
-// shared memory (mixed_cluster_kernel, run_cluster_big): the clusters take
-// the long items first, one per cluster, then every CTA takes short items on
-// its own.  Where the cluster form cannot be launched, the plain kernel runs
-// each long item on one CTA instead: the element-wise pre-processing, two
-// Stockham passes over global memory through the CTA's private scratch slice
-// and the post-processing.
+// complex points) run by default on one CTA each: the element-wise
+// pre-processing, two Stockham passes over global memory through the CTA's
+// private scratch slice and the post-processing.  With
+// MINFFT_B200_MIXED_CLUSTER=1 (where the device can co-schedule the clusters)
+// they run instead on clusters of eight CTAs entirely in distributed shared
+// memory (mixed_cluster_kernel, run_cluster_big): the clusters take the long
+// items first, one per cluster, then every CTA takes short items on its own.
+// That form moves each element through HBM once but measured slower.
 //
 // No CTA ever waits on a CTA outside its own cluster (the queues are a
 // single atomicAdd per item; the CTAs of a cluster are co-resident by
@@ -527,8 +528,29 @@ __device__ __forceinline__ void big_post_pair(const Params& mp, const Item& it, 
   }
 }
 
+// Row k1 of step 2 held by CTA `rank` at local index kk < K1.  The pairing
+// kinds (real DFT, DCT-2) need z_k beside z_{L-k}: with k = k1 + N1*k2, the
+// partner sits in row N1 - k1 (rows 0 and N1/2 are their own partners), so
+// their CTAs take the rows in mirrored pairs (base + p, N1 - base - p),
+// base = rank*K1/2 (CTA 0: rows 0 and N1/2, then its pairs) and every partner
+// is local.  The other kinds take K1 consecutive rows, so that their stores
+// run along k1.
+template <int N1, int K1>
+__device__ __forceinline__ int step2_row(bool pairs, int rank, int kk) {
+  if (!pairs) return rank * K1 + kk;
+  const int p = kk >> 1, base = rank * (K1 / 2);
+  if (rank == 0 && p == 0) return (kk & 1) ? N1 / 2 : 0;
+  return (kk & 1) ? N1 - (base + p) : base + p;
+}
+
+// One long item on the cluster.  Two cluster barriers: after step 1 (every
+// CTA's columns are in its tile) and after the gather of step 2 (no CTA reads
+// another's tile any more, so each may overwrite its own, for step 2's
+// exchanges and for the next item).  `next` is the index of the cluster's next
+// item, which cluster rank 0 has written to its slot before this item began;
+// it is read once the first barrier has made it visible.
 template <int LG>
-__device__ __noinline__ void run_cluster_big(const Params& mp, const Item& it, unsigned char* smem) {
+__device__ __noinline__ int run_cluster_big(const Params& mp, const Item& it, unsigned char* smem, const int* next) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   constexpr int L = 1 << LG;
@@ -538,7 +560,7 @@ __device__ __noinline__ void run_cluster_big(const Params& mp, const Item& it, u
   constexpr int K1 = N1 / kCluster;           // rows k1 per CTA in step 2: 8, 16, 32
   constexpr int TPT2 = kThreads / K1;         // 64, 32, 16
   constexpr int R2 = kN2 / TPT2;              // 4, 8, 16
-  static_assert(R1 >= 4 && R2 >= 4 && TPT1 * kColsPerCta == kThreads, "shape");
+  static_assert(R1 >= 4 && R2 >= 4 && TPT1 * kColsPerCta == kThreads && K1 >= 4, "shape");
   const int rank = int(cl.block_rank());
   const Job job = mp.jobs[mp.order[it.first]];
   cpx* tile = reinterpret_cast<cpx*>(smem + kOffsetsBytes);
@@ -546,6 +568,7 @@ __device__ __noinline__ void run_cluster_big(const Params& mp, const Item& it, u
   const int lp2 = tile_pitch(kN2, R2, K1, 1);
   const int lobits = (LG + 1) / 2;
   const int64_t lomask = (int64_t(1) << lobits) - 1;
+  const bool pairs = it.combo == K_R2C || it.combo == K_DCT2;
 
   // ---- step 1: DFTs over n1 of the columns n2 = 32*rank + c
   {
@@ -566,10 +589,11 @@ __device__ __noinline__ void run_cluster_big(const Params& mp, const Item& it, u
     scatter_natural<N1, R1>(v, j, c, t);
   }
   cl.sync();
+  const int nxt = *cl.map_shared_rank(next, 0);
 
-  // ---- step 2: DFTs over n2 of the rows k1 = rank*K1 + kk
+  // ---- step 2: DFTs over n2 of the CTA's K1 rows
   const int kk = threadIdx.x % K1, j2 = threadIdx.x / K1;
-  const int k1 = rank * K1 + kk;
+  const int k1 = step2_row<N1, K1>(pairs, rank, kk);
   cpx v[R2];
 #pragma unroll
   for (int r = 0; r < R2; ++r) {
@@ -581,10 +605,12 @@ __device__ __noinline__ void run_cluster_big(const Params& mp, const Item& it, u
   Tile t2{tile, lp2};
   run_passes<kN2, R2, 1>(v, j2, kk, t2, mp.tw[log2c(kN2)]);
   // v[r] = z_k, k = k1 + N1*k2, k2 = j2 + r*TPT2
-  if (it.combo == K_R2C || it.combo == K_DCT2) {
+  if (pairs) {
     __syncthreads();
     scatter_natural<kN2, R2>(v, j2, kk, t2);
-    cl.sync();
+    __syncthreads();
+    // partner row: the other member of the pair (rows 0 and N1/2: the row itself)
+    const int pkk = (rank == 0 && kk < 2) ? kk : (kk ^ 1);
 #pragma unroll
     for (int r = 0; r < R2; ++r) {
       const int k2 = j2 + r * TPT2;
@@ -592,10 +618,8 @@ __device__ __noinline__ void run_cluster_big(const Params& mp, const Item& it, u
       if (2 * k > L) continue;
       cpx zb = czero();
       if (k != 0 && 2 * k != L) {
-        const int pk1 = k1 == 0 ? 0 : N1 - k1;
         const int pk2 = k1 == 0 ? kN2 - k2 : kN2 - 1 - k2;
-        const cpx* src = cl.map_shared_rank(tile, pk1 / K1);
-        zb = src[(pk1 % K1) * lp2 + pad16(pk2)];
+        zb = tile[pkk * lp2 + pad16(pk2)];
       }
       big_post_pair(mp, it, job, LG, k, v[r], zb);
     }
@@ -603,7 +627,8 @@ __device__ __noinline__ void run_cluster_big(const Params& mp, const Item& it, u
 #pragma unroll
     for (int r = 0; r < R2; ++r) big_post_single(mp, it, job, LG, int64_t(k1) + int64_t(N1) * (j2 + r * TPT2), v[r]);
   }
-  cl.sync();  // the tile and the item slot may be reused
+  __syncthreads();  // the local tile may be reused
+  return nxt;
 }
 
 // Shared memory a CTA needs for its part of a long item.
@@ -628,17 +653,21 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<16>::value) mixed_cluster_
   namespace cg = cooperative_groups;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_item;
+  __shared__ int s_next[2];  // cluster rank 0: the cluster's next long item, by item parity
   cg::cluster_group cl = cg::this_cluster();
-  for (;;) {
-    if (cl.block_rank() == 0 && threadIdx.x == 0) s_item = int(atomicAdd(mp.counter + 1, 1u));
-    cl.sync();
-    const int idx = *cl.map_shared_rank(&s_item, 0);
-    if (idx >= mp.nbig) break;
+  const bool lead = cl.block_rank() == 0 && threadIdx.x == 0;
+  if (lead) s_next[0] = int(atomicAdd(mp.counter + 1, 1u));
+  cl.sync();
+  int idx = *cl.map_shared_rank(&s_next[0], 0);
+  for (int n = 0; idx < mp.nbig; ++n) {
+    // the index after this one, read by the cluster after this item's first
+    // barrier (the slot it replaces was read during the previous item)
+    if (lead) s_next[(n + 1) & 1] = int(atomicAdd(mp.counter + 1, 1u));
     const Item it = mp.items[idx];
     switch (it.log2L) {
-      case 14: run_cluster_big<14>(mp, it, smem); break;
-      case 15: run_cluster_big<15>(mp, it, smem); break;
-      default: run_cluster_big<16>(mp, it, smem); break;
+      case 14: idx = run_cluster_big<14>(mp, it, smem, &s_next[(n + 1) & 1]); break;
+      case 15: idx = run_cluster_big<15>(mp, it, smem, &s_next[(n + 1) & 1]); break;
+      default: idx = run_cluster_big<16>(mp, it, smem, &s_next[(n + 1) & 1]); break;
     }
   }
   cl.sync();  // rank 0's slot has been read by all before anyone moves on
@@ -929,8 +958,10 @@ MB_EXPORT minfft_b200_mixed* minfft_b200_mixed_plan(int count, const minfft_b200
     if (lgL > kSmallMaxLog2L) {
       max_big = std::max(max_big, lgL);
       need_st[lgL] = 1;
-      need_tw[(lgL + 1) / 2] = 1;
+      need_tw[(lgL + 1) / 2] = 1;  // scratch form: its two passes
       need_tw[lgL - (lgL + 1) / 2] = 1;
+      need_tw[lgL - ilog2i(kN2)] = 1;  // cluster form: the L/256-point column DFTs
+      need_tw[ilog2i(kN2)] = 1;        // and the 256-point row DFTs
     } else {
       need_tw[lgL] = 1;
     }
@@ -1049,11 +1080,15 @@ MB_EXPORT int minfft_b200_mixed_autotune(minfft_b200_mixed* m, int reps) {
   float best = 1e30f;
   int best_split = m->split, best_per = m->per_sm;
   const int grid_cap = m->grid;  // scratch is sized for this many CTAs
+  // the cluster form keeps every co-resident cluster (its grid is the
+  // occupancy query's cluster count, not a multiple of the SMs)
+  auto grid_for = [&](int per) {
+    return m->cluster ? grid_cap : std::min(grid_cap, sms * per);
+  };
   for (int split : {1, 2, 4, 8}) {
-    for (int per = 1; per <= max_per_sm; ++per) {
+    for (int per = 1; per <= (m->cluster ? 1 : max_per_sm); ++per) {
       m->split = split;
-      m->grid = std::min(grid_cap, sms * per);
-      if (m->cluster) m->grid = std::max(kCluster, m->grid / kCluster * kCluster);
+      m->grid = grid_for(per);
       if (!build_items(m)) continue;
       cudaGraphLaunch(m->exec, st);
       cudaEventRecord(e0, st);
@@ -1072,7 +1107,6 @@ MB_EXPORT int minfft_b200_mixed_autotune(minfft_b200_mixed* m, int reps) {
   cudaEventDestroy(e1);
   cudaStreamDestroy(st);
   m->split = best_split;
-  m->grid = std::min(grid_cap, sms * best_per);
-  if (m->cluster) m->grid = std::max(kCluster, m->grid / kCluster * kCluster);
+  m->grid = grid_for(best_per);
   return build_items(m) ? MINFFT_B200_OK : MINFFT_B200_ECUDA;
 }

@@ -149,3 +149,25 @@ def test_mixed_cluster_form_every_long_kind(single, monkeypatch):
         check_batch(single, pool, host)
     finally:
         eng.mixed_free(h)
+
+
+@pytest.mark.parametrize("cluster", ["0", "1"], ids=["scratch", "cluster"])
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+def test_mixed_long_items_only(single, cluster, monkeypatch):
+    """A batch of long items and nothing else: every root table the long
+    items read (the scratch form's two pass lengths, the cluster form's
+    L/256- and 256-point DFTs) is built from the long items themselves, not
+    borrowed from short items of those lengths."""
+    monkeypatch.setenv("MINFFT_B200_MIXED_CLUSTER", cluster)
+    rng = np.random.default_rng(23)
+    specs = [("dft", 1 << 14)] * 3 + [("invdft", 1 << 15)] * 2 + [("dft", 1 << 16)] + [("realdft", 1 << 15)] + \
+            [("dct2", 1 << 16)] + [("dst4", 1 << 17)]
+    eng = minfft_b200.engine(single)
+    pool, jobs, host = make_batch(single, specs, rng)
+    h = eng.mixed_plan(jobs)
+    try:
+        eng.mixed_execute(h)
+        torch.cuda.synchronize()
+        check_batch(single, pool, host)
+    finally:
+        eng.mixed_free(h)
