@@ -735,34 +735,55 @@ struct LoadDCT3 {
 // DCT-4, -w_2N^g (x[2g] - i x[N-1-2g]) for DST-4, x the line's N = kn reals
 // at b2 * k_in_line.  w_2N^g is the product of the coarse and fine roots
 // (st_hi, st_lo, st_lobits) of 2N: the first pass has no pre-twiddle of its
-// own.  Each real is read once overall: x[2g] here, its neighbour x[2g+1]
-// by element N/2-1-g.
+// own.  The CTA holds mirror pairs of sub-DFTs (MirrorPairs below): point
+// g's mirror Lt-1-g (Lt = N/2) is element L-1-n of the partner sub-DFT, and
+// x[2g+1] = x[N-1-2(Lt-1-g)].  So each element reads the real pair
+// (x[2g], x[2g+1]) as one vector, keeps x[2g] and hands x[2g+1] to its
+// mirror element's thread through the tile: every real is read once, in
+// whole sectors.
 struct LoadT4Chain {
   static constexpr bool kComplexIn = false;  // whether the raw input elements are complex
   static constexpr bool kStaged = false;
   template <int L, int R>
-  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
     constexpr int TPT = L / R;
-    if (!x.active) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = czero();
-      return;
-    }
     const int64_t rest = x.b / p.d0;
     const int64_t b1 = rest % p.d1, b2 = rest / p.d1;
     const real* in = static_cast<const real*>(p.in) + b2 * p.k_in_line;
-    const int64_t N = p.kn;
     const bool dst = (p.flags & F_DST) != 0;
     const int64_t lomask = (int64_t(1) << p.st_lobits) - 1;
+    const int h = p.cpb / 2;
+    const int pc = x.c < h ? x.c + h : x.c - h;  // the mirror sub-DFT's slot
+    real* sb = reinterpret_cast<real*>(t.s);
+    const bool vec = (reinterpret_cast<uintptr_t>(in) % sizeof(cpx)) == 0;
+    real a[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int64_t g = b1 * p.is1 + int64_t(x.j + r * TPT) * p.in_n;
-      const real a = in[2 * g], b = in[N - 1 - 2 * g];
+      const int n = x.j + r * TPT;
+      const int64_t g = b1 * p.is1 + int64_t(n) * p.in_n;
+      real lo, hi;
+      if (vec) {
+        const cpx q = __ldcs(reinterpret_cast<const cpx*>(in + 2 * g));
+        lo = q.x;
+        hi = q.y;
+      } else {
+        lo = __ldcs(in + 2 * g);
+        hi = __ldcs(in + 2 * g + 1);
+      }
+      a[r] = lo;
+      sb[pc * 2 * t.lp + (L - 1 - n)] = hi;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int n = x.j + r * TPT;
+      const int64_t g = b1 * p.is1 + int64_t(n) * p.in_n;
+      const real b = sb[x.c * 2 * t.lp + n];
       const cpx e = cmul(ldg(p.st_hi + (g >> p.st_lobits)), ldg(p.st_lo + (g & lomask)));
       if (!dst) {
-        v[r] = cmul(e, cmk(a, b));
+        v[r] = cmul(e, cmk(a[r], b));
       } else {
-        const cpx q = cmul(e, cmk(a, -b));
+        const cpx q = cmul(e, cmk(a[r], -b));
         v[r] = cmk(-q.x, -q.y);
       }
     }
@@ -1071,34 +1092,87 @@ struct StoreT4 {
 // sub-DFT b is the line's point m = (its normal offset) + k*out_k, and
 // T_m gives y[2m] = 2 Re(g_2m T_m), y[N-1-2m] = 2 Re(g_{N-1-2m} conj(T_m))
 // (Im for DST-4), g_q = w_8N^(2q+1) as the product of the coarse and fine
-// roots t1, t2 of 8N (kbits fine bits); y is the line's N reals at
-// b2 * k_out_line (the pass's os2 is 0).
+// roots t1, t2 of 8N (kbits fine bits), and g_{N-1-2m} = -i conj(g_2m); y is
+// the line's N reals at b2 * k_out_line (the pass's os2 is 0).  As in
+// LoadT4Chain the CTA holds mirror pairs of sub-DFTs: y[2m+1] is
+// y[N-1-2m'] of the mirror point m' = Lt-1-m (output L-1-k of the partner
+// sub-DFT), so each element hands that value to its mirror's thread through
+// the tile and writes the pair (y[2m], y[2m+1]) as one vector.
 struct StoreT4Chain {
   template <int L, int R>
-  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, const TileOffsets&,
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, const TileOffsets&,
                                              cpx (&v)[R]) {
-    if (!x.active) return;
     constexpr int TPT = L / R;
     const int64_t b2 = x.b / (p.d0 * p.d1);
     real* out = static_cast<real*>(p.out) + b2 * p.k_out_line;
-    const int64_t N = p.kn;
     const bool dst = (p.flags & F_DST) != 0;
     const int64_t lomask = (int64_t(1) << p.kbits) - 1;
-    auto g = [&](int64_t q) {
-      const int64_t e = 2 * q + 1;
-      return cmul(ldg(p.t1 + (e >> p.kbits)), ldg(p.t2 + (e & lomask)));
-    };
+    const int h = p.cpb / 2;
+    const int pc = x.c < h ? x.c + h : x.c - h;  // the mirror sub-DFT's slot
+    real* sb = reinterpret_cast<real*>(t.s);
+    const bool vec = (reinterpret_cast<uintptr_t>(out) % sizeof(cpx)) == 0;
+    real own[R];
+    __syncthreads();  // the last Stockham exchange has finished with the tile
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int64_t m = x.oout + int64_t(x.j + r * TPT) * p.out_k;
+      const int k = x.j + r * TPT;
+      const int64_t m = x.oout + int64_t(k) * p.out_k;
+      const int64_t e = 4 * m + 1;
+      const cpx ga = cmul(ldg(p.t1 + (e >> p.kbits)), ldg(p.t2 + (e & lomask)));
+      const cpx gb = cmk(-ga.y, -ga.x);  // -i conj(ga) = w_8N^(2N-1-4m)
       const cpx T = v[r];
-      const cpx a = cmul(g(2 * m), T);
-      const cpx b = cmul(g(N - 1 - 2 * m), cconj(T));
-      out[2 * m] = 2 * (dst ? a.y : a.x);
-      out[N - 1 - 2 * m] = 2 * (dst ? b.y : b.x);
+      const cpx A = cmul(ga, T);
+      const cpx B = cmul(gb, cconj(T));
+      own[r] = 2 * (dst ? A.y : A.x);
+      sb[pc * 2 * t.lp + (L - 1 - k)] = 2 * (dst ? B.y : B.x);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int k = x.j + r * TPT;
+      const int64_t m = x.oout + int64_t(k) * p.out_k;
+      const real part = sb[x.c * 2 * t.lp + k];
+      if (vec) {
+        __stcs(reinterpret_cast<cpx*>(out + 2 * m), cmk(own[r], part));
+      } else {
+        __stcs(out + 2 * m, own[r]);
+        __stcs(out + 2 * m + 1, part);
+      }
     }
   }
 };
+
+// The fused type-4 passes take mirror pairs of sub-DFTs into one CTA: with
+// M = d0*d1 sub-DFTs per line, slots c < cpb/2 hold sub-DFTs i of the line
+// and slots c + cpb/2 their mirrors M-1-i (the planner makes cpb even and a
+// divisor of M).
+template <class Op>
+struct MirrorPairs {
+  static constexpr bool value = false;
+};
+template <>
+struct MirrorPairs<LoadT4Chain> {
+  static constexpr bool value = true;
+};
+template <>
+struct MirrorPairs<StoreT4Chain> {
+  static constexpr bool value = true;
+};
+
+// Batch index of the CTA's transform in slot c.
+template <bool kMirror>
+__device__ __forceinline__ int64_t tile_batch(const AxisParams& p, int c) {
+  if constexpr (kMirror) {
+    const int64_t M = p.d0 * p.d1;
+    const int64_t per_line = M / p.cpb;  // CTAs per line
+    const int64_t line = int64_t(blockIdx.x) / per_line, q = int64_t(blockIdx.x) % per_line;
+    const int h = p.cpb / 2;
+    const int64_t i = q * h + (c < h ? c : c - h);
+    return line * M + (c < h ? i : M - 1 - i);
+  } else {
+    return int64_t(blockIdx.x) * p.cpb + c;
+  }
+}
 
 // ------------------------------------------------------------------ kernel
 // Register budget per thread: a radix-R thread holds R complex values; with
@@ -1123,9 +1197,10 @@ __global__ void __launch_bounds__(512, MinBlocks<R>::value) axis_pass_kernel(con
   TileOffsets to{offs, offs + p.cpb, int(left < p.cpb ? left : p.cpb)};
   Tile t{reinterpret_cast<cpx*>(smem_raw + 16 * ((2 * p.cpb * sizeof(int64_t) + 15) / 16)), p.lp};
 
+  constexpr bool kMirror = MirrorPairs<LoadOp>::value || MirrorPairs<StoreOp>::value;
   // offsets of the CTA's transforms, computed once per transform
   for (int c = threadIdx.x; c < p.cpb; c += blockDim.x) {
-    const int64_t b = int64_t(blockIdx.x) * p.cpb + c;
+    const int64_t b = tile_batch<kMirror>(p, c);
     int64_t b0, oi, oo;
     batch_offsets(p, b < p.nbatch ? b : 0, b0, oi, oo);
     to.in_off[c] = oi;
@@ -1141,7 +1216,7 @@ __global__ void __launch_bounds__(512, MinBlocks<R>::value) axis_pass_kernel(con
     x.j = threadIdx.x % TPT;
     x.c = threadIdx.x / TPT;
   }
-  x.b = int64_t(blockIdx.x) * p.cpb + x.c;
+  x.b = tile_batch<kMirror>(p, x.c);
   x.active = x.b < p.nbatch;
   x.oin = to.in_off[x.c];
   x.oout = to.out_off[x.c];

@@ -422,6 +422,17 @@ constexpr int kRowCapLog2 = 13;  // in-CTA DFT along contiguous rows: <= 8192
 constexpr int kColCapLog2 = 12;  // along strided columns: <= 4096
 constexpr int kPassCapLog2 = 12; // sub-DFTs of the HBM passes: <= 4096
 
+// Longest sub-DFT of an HBM pass (log2): kPassCapLog2 unless
+// MINFFT_B200_PASS_CAP (8 .. 12) sets another, for measurement.
+int pass_cap_log2() {
+  static const int v = [] {
+    const char* e = getenv("MINFFT_B200_PASS_CAP");
+    const int c = e ? atoi(e) : 0;
+    return (c >= 8 && c <= kPassCapLog2) ? c : kPassCapLog2;
+  }();
+  return v;
+}
+
 struct AxisStep {
   int combo;        // mb::Combo
   int64_t N;        // axis length (real length for real kinds)
@@ -459,10 +470,15 @@ struct Planner {
     return cpb;
   }
 
+  // kinds whose load or store stage uses the shared-memory tile (the fused
+  // type-4 passes hand each real pair's second value to the mirror element)
   static bool staged(int combo) {
     return combo == mb::K_R2C || combo == mb::K_C2R || combo == mb::K_DCT2 || combo == mb::K_DCT3 ||
-           combo == mb::K_R2CQ || combo == mb::K_C2RQ;
+           combo == mb::K_R2CQ || combo == mb::K_C2RQ || combo == mb::K_T4IN || combo == mb::K_T4OUT;
   }
+
+  // the fused type-4 passes hold mirror pairs of sub-DFTs in one CTA
+  static bool mirror_pairs(int combo) { return combo == mb::K_T4IN || combo == mb::K_T4OUT; }
 
   // the split-column kinds work on exactly four rows per CTA
   static bool four_rows(int combo) { return combo == mb::K_R2CQ || combo == mb::K_C2RQ; }
@@ -501,7 +517,7 @@ struct Planner {
     const size_t sm =
         tile ? mb::axis_pass_smem(L, Re, cpb, colmode) : size_t(16 * ((2 * cpb * sizeof(int64_t) + 15) / 16));
     return mb::axis_kernel(combo, ilog2(L), R) && cpb >= 1 && cpb <= max_threads_cpb(L, R) &&
-           sm <= (size_t)dev_max_smem;
+           (!mirror_pairs(combo) || cpb % 2 == 0) && sm <= (size_t)dev_max_smem;
   }
 
   // The tensor-core pass covers complex 256-point axes: every in-CTA axis
@@ -533,7 +549,7 @@ struct Planner {
     if (a->precision != MINFFT_B200_PREC_FP32) {
       for (k = std::min(P, bits / tb); k > 0; --k) {
         const int rest = bits - tb * k, left = P - k;
-        if (left == 0 ? rest == 0 : (rest >= left && rest <= left * kPassCapLog2)) break;
+        if (left == 0 ? rest == 0 : (rest >= left && rest <= left * pass_cap_log2())) break;
       }
     }
     std::vector<int> pb(k, tb);
@@ -805,6 +821,18 @@ struct Planner {
     if (four_rows(combo)) {
       ap.cpb = 4;
       if (!mb::axis_kernel(combo, lg, R)) R = (R == 16) ? 8 : 16;
+    }
+    if (mirror_pairs(combo)) {
+      // an even tile that divides the M sub-DFTs of a line (mirror i and M-1-i)
+      const int64_t M = ap.d0 * ap.d1;
+      if (ap.cpb < 2) ap.cpb = 2;
+      while (ap.cpb > 2 && M % ap.cpb) ap.cpb /= 2;
+      if (M % ap.cpb || nbatch % M || ap.cpb * (L / std::min(R, L)) > 512) {
+        set_error(MINFFT_B200_EUNSUPPORTED, "no mirror-pair tile for the type-4 pass (L=%d, %lld sub-DFTs per line)",
+                  L, (long long)M);
+        ok = false;
+        return;
+      }
     }
     Launch ln;
     ln.key = key;
@@ -1464,7 +1492,7 @@ struct Planner {
   // Stockham FFT over HBM for a long axis (see the file comment).
   void plan_multipass(const AxisStep& s, int64_t Lt) {
     const int bits = ilog2(Lt);
-    int P = (bits + kPassCapLog2 - 1) / kPassCapLog2;
+    int P = (bits + pass_cap_log2() - 1) / pass_cap_log2();
     std::vector<int> pb = pass_bits(bits, P);
     // a tensor-core mode whose chain has no 256-point pass at the FP32 pass
     // count (2^17 .. 2^24 points in two passes) takes one more pass so that
