@@ -420,17 +420,25 @@ const cpx* table(minfft_aux* a, int kind, int64_t N) {
 // ------------------------------------------------------------ planner
 constexpr int kRowCapLog2 = 13;  // in-CTA DFT along contiguous rows: <= 8192
 constexpr int kColCapLog2 = 12;  // along strided columns: <= 4096
-constexpr int kPassCapLog2 = 12; // sub-DFTs of the HBM passes: <= 4096
+constexpr int kPassCapLog2 = 12;    // sub-DFTs of the HBM passes: <= 4096
+constexpr int kPassCapLog2Cc = 10;  // ... of the CUDA-core (FP32/FP64) chains: <= 1024
 
-// Longest sub-DFT of an HBM pass (log2): kPassCapLog2 unless
-// MINFFT_B200_PASS_CAP (8 .. 12) sets another, for measurement.
-int pass_cap_log2() {
-  static const int v = [] {
+// Longest sub-DFT of an HBM pass (log2).  A column pass over HBM holds at
+// most 512/(L/16) sub-DFTs per CTA, so lengths of 2048 and 4096 leave two to
+// four adjacent columns per CTA (runs of 16-64 bytes per row) and ran at half
+// the bandwidth of passes of 1024 points or fewer: the CUDA-core chains take
+// a third pass instead (2^21 .. 2^24 points; the f32 2^24 DCT-4 + DST-4 step
+// went from 0.350 to 0.238 ms).  Tensor-core chains are built around their
+// 256-point passes and keep 4096.  MINFFT_B200_PASS_CAP (8 .. 12) overrides
+// both, for measurement.
+int pass_cap_log2(int precision) {
+  static const int forced = [] {
     const char* e = getenv("MINFFT_B200_PASS_CAP");
     const int c = e ? atoi(e) : 0;
-    return (c >= 8 && c <= kPassCapLog2) ? c : kPassCapLog2;
+    return (c >= 8 && c <= kPassCapLog2) ? c : 0;
   }();
-  return v;
+  if (forced) return forced;
+  return precision == MINFFT_B200_PREC_FP32 ? kPassCapLog2Cc : kPassCapLog2;
 }
 
 struct AxisStep {
@@ -549,7 +557,7 @@ struct Planner {
     if (a->precision != MINFFT_B200_PREC_FP32) {
       for (k = std::min(P, bits / tb); k > 0; --k) {
         const int rest = bits - tb * k, left = P - k;
-        if (left == 0 ? rest == 0 : (rest >= left && rest <= left * pass_cap_log2())) break;
+        if (left == 0 ? rest == 0 : (rest >= left && rest <= left * pass_cap_log2(a->precision))) break;
       }
     }
     std::vector<int> pb(k, tb);
@@ -1492,7 +1500,8 @@ struct Planner {
   // Stockham FFT over HBM for a long axis (see the file comment).
   void plan_multipass(const AxisStep& s, int64_t Lt) {
     const int bits = ilog2(Lt);
-    int P = (bits + pass_cap_log2() - 1) / pass_cap_log2();
+    const int cap = pass_cap_log2(a->precision);
+    int P = (bits + cap - 1) / cap;
     std::vector<int> pb = pass_bits(bits, P);
     // a tensor-core mode whose chain has no 256-point pass at the FP32 pass
     // count (2^17 .. 2^24 points in two passes) takes one more pass so that
