@@ -339,6 +339,42 @@ __device__ __forceinline__ void col_g2s(real* sr, const real* g, int64_t s, int 
 __device__ __forceinline__ bool rows_staged_in(const AxisParams& p) { return !p.colmode && p.in_n == 1; }
 __device__ __forceinline__ bool rows_staged_out(const AxisParams& p) { return !p.colmode && p.out_k == 1; }
 
+// ------------------------------------------------- root progressions
+// W^(g0 + r*D), r < R, for the root table pair (hi, lo) of W: each table
+// root is hi[e >> lobits] * lo[e & (2^lobits - 1)].  Three table roots per
+// thread (W^g0, W^D, W^4D); at(r) forms the rest as at most two products, as
+// the Stockham passes form theirs (apply_root_powers), just before use so
+// that only the seven factors stay live.  Every exponent g0 + r*D must lie
+// inside the tables; exponents are 32-bit (the planner keeps the tables
+// below 2^32 roots).
+template <int R>
+struct RootProgression {
+  cpx base, d1, d2, d3, d4, d8, d12;
+  __device__ __forceinline__ RootProgression(const cpx* __restrict__ hi, const cpx* __restrict__ lo, int lobits,
+                                             uint32_t g0, uint32_t D) {
+    const uint32_t lomask = (1u << lobits) - 1u;
+    auto root = [&](uint32_t e) { return cmul(ldg(hi + (e >> lobits)), ldg(lo + (e & lomask))); };
+    base = root(g0);
+    d1 = R > 1 ? root(D) : czero();
+    d2 = cmul(d1, d1);
+    d3 = cmul(d2, d1);
+    d4 = R > 4 ? root(4 * D) : czero();
+    d8 = cmul(d4, d4);
+    d12 = cmul(d8, d4);
+  }
+  __device__ __forceinline__ cpx at(int r) const {
+    const int lo2 = r & 3, hi2 = r >> 2;
+    cpx t = base;
+    if (hi2 == 1) t = cmul(t, d4);
+    if (hi2 == 2) t = cmul(t, d8);
+    if (hi2 == 3) t = cmul(t, d12);
+    if (lo2 == 1) t = cmul(t, d1);
+    if (lo2 == 2) t = cmul(t, d2);
+    if (lo2 == 3) t = cmul(t, d3);
+    return t;
+  }
+};
+
 // ------------------------------------------------------- HBM pre-twiddle
 // In a pass of a Stockham FFT over HBM, element n of a sub-DFT with span
 // index q is multiplied by w_Lt^g, g = q*n*Lt/(st_ns*L), each root read as
@@ -751,7 +787,6 @@ struct LoadT4Chain {
     const int64_t b1 = rest % p.d1, b2 = rest / p.d1;
     const real* in = static_cast<const real*>(p.in) + b2 * p.k_in_line;
     const bool dst = (p.flags & F_DST) != 0;
-    const int64_t lomask = (int64_t(1) << p.st_lobits) - 1;
     const int h = p.cpb / 2;
     const int pc = x.c < h ? x.c + h : x.c - h;  // the mirror sub-DFT's slot
     real* sb = reinterpret_cast<real*>(t.s);
@@ -774,12 +809,14 @@ struct LoadT4Chain {
       sb[pc * 2 * t.lp + (L - 1 - n)] = hi;
     }
     __syncthreads();
+    // w_2N^g for g = g0 + r*TPT*in_n
+    const RootProgression<R> ew(p.st_hi, p.st_lo, p.st_lobits, uint32_t(b1 * p.is1 + int64_t(x.j) * p.in_n),
+                                uint32_t(int64_t(TPT) * p.in_n));
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int n = x.j + r * TPT;
-      const int64_t g = b1 * p.is1 + int64_t(n) * p.in_n;
       const real b = sb[x.c * 2 * t.lp + n];
-      const cpx e = cmul(ldg(p.st_hi + (g >> p.st_lobits)), ldg(p.st_lo + (g & lomask)));
+      const cpx e = ew.at(r);
       if (!dst) {
         v[r] = cmul(e, cmk(a[r], b));
       } else {
@@ -1106,24 +1143,24 @@ struct StoreT4Chain {
     const int64_t b2 = x.b / (p.d0 * p.d1);
     real* out = static_cast<real*>(p.out) + b2 * p.k_out_line;
     const bool dst = (p.flags & F_DST) != 0;
-    const int64_t lomask = (int64_t(1) << p.kbits) - 1;
     const int h = p.cpb / 2;
     const int pc = x.c < h ? x.c + h : x.c - h;  // the mirror sub-DFT's slot
     real* sb = reinterpret_cast<real*>(t.s);
     const bool vec = (reinterpret_cast<uintptr_t>(out) % sizeof(cpx)) == 0;
-    real own[R];
+    // g_2m = w_8N^(4m+1) for m = m0 + r*TPT*out_k
+    const RootProgression<R> gw(p.t1, p.t2, p.kbits, uint32_t(4 * (x.oout + int64_t(x.j) * p.out_k) + 1),
+                                uint32_t(4 * int64_t(TPT) * p.out_k));
     __syncthreads();  // the last Stockham exchange has finished with the tile
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int k = x.j + r * TPT;
-      const int64_t m = x.oout + int64_t(k) * p.out_k;
-      const int64_t e = 4 * m + 1;
-      const cpx ga = cmul(ldg(p.t1 + (e >> p.kbits)), ldg(p.t2 + (e & lomask)));
+      const cpx ga = gw.at(r);
       const cpx gb = cmk(-ga.y, -ga.x);  // -i conj(ga) = w_8N^(2N-1-4m)
       const cpx T = v[r];
       const cpx A = cmul(ga, T);
       const cpx B = cmul(gb, cconj(T));
-      own[r] = 2 * (dst ? A.y : A.x);
+      // a slot holds 2*lp >= 2L reals: the mirror's values below L, its own above
+      sb[x.c * 2 * t.lp + L + k] = 2 * (dst ? A.y : A.x);
       sb[pc * 2 * t.lp + (L - 1 - k)] = 2 * (dst ? B.y : B.x);
     }
     __syncthreads();
@@ -1131,11 +1168,12 @@ struct StoreT4Chain {
     for (int r = 0; r < R; ++r) {
       const int k = x.j + r * TPT;
       const int64_t m = x.oout + int64_t(k) * p.out_k;
+      const real own = sb[x.c * 2 * t.lp + L + k];
       const real part = sb[x.c * 2 * t.lp + k];
       if (vec) {
-        __stcs(reinterpret_cast<cpx*>(out + 2 * m), cmk(own[r], part));
+        __stcs(reinterpret_cast<cpx*>(out + 2 * m), cmk(own, part));
       } else {
-        __stcs(out + 2 * m, own[r]);
+        __stcs(out + 2 * m, own);
         __stcs(out + 2 * m + 1, part);
       }
     }

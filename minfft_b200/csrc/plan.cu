@@ -1537,8 +1537,9 @@ struct Planner {
     // A 1-D type-4 chain of two or more passes in FP32 fuses its pre-rotation
     // into the first pass's load and its post-rotation into the last pass's
     // store (LoadT4Chain, StoreT4Chain): two passes over HBM instead of four.
+    // (the fused passes form their roots from 32-bit exponents into the tables of 8N)
     const bool t4_fused = s.combo == mb::K_T4 && inner == 1 && P >= 2 && a->precision == MINFFT_B200_PREC_FP32 &&
-                          t4_fuse_enabled();
+                          s.N <= (int64_t(1) << 28) && t4_fuse_enabled();
     if (!t4_fused &&
         (s.combo == mb::K_DCT2 || s.combo == mb::K_T4 || s.combo == mb::K_C2R || s.combo == mb::K_DCT3)) {
       cs = BUF_T2;

@@ -107,6 +107,32 @@ def test_fused_type4_chain_matches_oracle(single):
 
 
 @pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+def test_fused_type4_chain_with_offset_arrays(single):
+    """Real arrays that start one element past a complex boundary: the fused
+    type-4 passes read and write their real pairs as two scalars instead of
+    one vector (LoadT4Chain, StoreT4Chain), with the same results."""
+    eng = minfft_b200.engine(single)
+    rng = np.random.default_rng(64)
+    tdt = torch.float32 if single else torch.float64
+    for dims in [(1 << 17,), (2, 1 << 15)]:
+        for op in ("dct4", "dst4"):
+            x = make_input(op, dims, rng, single)
+            n = x.size
+            src = torch.zeros(n + 1, dtype=tdt, device="cuda")
+            src[1:] = torch.from_numpy(x.ravel()).cuda()
+            dst = torch.zeros(n + 1, dtype=tdt, device="cuda")
+            plan = eng.plan("t4", dims)
+            try:
+                esz = src.element_size()
+                plan(op, src.data_ptr() + esz, dst.data_ptr() + esz)
+                torch.cuda.synchronize()
+            finally:
+                plan.free()
+            err = rel_l2(dst[1:].cpu().numpy().reshape(dims), expected(op, x, dims))
+            assert err <= tolerance(single, dims), (op, dims, err)
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
 @pytest.mark.parametrize("form,cpb", [(3, 0), (3, 1), (4, 2), (4, 8)])
 def test_streamed_rows_match_oracle(single, form, cpb):
     """The streamed row pass (bulk row copies into mbarrier stages, each
