@@ -136,10 +136,10 @@ struct Ctx {
 };
 
 __device__ __forceinline__ void batch_offsets(const AxisParams& p, int64_t b, int64_t& b0, int64_t& oi, int64_t& oo) {
-  b0 = b % p.d0;
-  const int64_t r = b / p.d0;
-  const int64_t b1 = r % p.d1;
-  const int64_t b2 = r / p.d1;
+  const int64_t r = udiv(b, p.d0);
+  b0 = b - r * p.d0;
+  const int64_t b2 = udiv(r, p.d1);
+  const int64_t b1 = r - b2 * p.d1;
   oi = b0 * p.is0 + b1 * p.is1 + b2 * p.is2;
   oo = b0 * p.os0 + b1 * p.os1 + b2 * p.os2;
 }
@@ -386,7 +386,7 @@ struct RootProgression {
 template <int L, int R>
 __device__ __forceinline__ void hbm_pretwiddle(cpx (&v)[R], const AxisParams& p, int64_t b0, int j) {
   constexpr int TPT = L / R;
-  const int64_t q = (b0 / p.st_div) & (p.st_ns - 1);
+  const int64_t q = udiv(b0, p.st_div) & (p.st_ns - 1);
   const int64_t lomask = (int64_t(1) << p.st_lobits) - 1;
   auto root = [&](int64_t g) { return cmul(ldg(p.st_hi + (g >> p.st_lobits)), ldg(p.st_lo + (g & lomask))); };
   if constexpr (R < 4) {
@@ -649,7 +649,7 @@ struct LoadC2RQ {
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
     constexpr int NT = 4 * (L / R);  // threads of the CTA (four transforms)
     const cpx* in = static_cast<const cpx*>(p.in) + (x.oin - int64_t(x.c) * p.is0);  // row j of block 0
-    const int64_t jr = (x.b / p.d0) % p.d1;  // the CTA's row index j
+    const int64_t jr = umod(udiv(x.b, p.d0), p.d1);  // the CTA's row index j
     const cpx w1 = cconj(ldg(p.t1 + jr)), w2 = cconj(ldg(p.t1 + 2 * jr)), w3 = cconj(ldg(p.t1 + 3 * jr));
     const int64_t bs = p.is0;
     // column col of the four blocks -> the four rows' spectra at col
@@ -783,8 +783,8 @@ struct LoadT4Chain {
   template <int L, int R>
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, cpx (&v)[R]) {
     constexpr int TPT = L / R;
-    const int64_t rest = x.b / p.d0;
-    const int64_t b1 = rest % p.d1, b2 = rest / p.d1;
+    const int64_t rest = udiv(x.b, p.d0);
+    const int64_t b2 = udiv(rest, p.d1), b1 = rest - b2 * p.d1;
     const real* in = static_cast<const real*>(p.in) + b2 * p.k_in_line;
     const bool dst = (p.flags & F_DST) != 0;
     const int h = p.cpb / 2;
@@ -972,7 +972,7 @@ struct StoreR2CQ {
     __syncthreads();
     scatter_natural<L, R>(v, x.j, x.c, t);
     __syncthreads();
-    const int64_t jr = (x.b / p.d0) % p.d1;  // the CTA's row index j
+    const int64_t jr = umod(udiv(x.b, p.d0), p.d1);  // the CTA's row index j
     const cpx w1 = ldg(p.t2 + jr), w2 = ldg(p.t2 + 2 * jr), w3 = ldg(p.t2 + 3 * jr);
     cpx* out = static_cast<cpx*>(p.out) + to.out_off[0];  // row j of block 0
     const int64_t bs = p.os0;
@@ -1140,7 +1140,7 @@ struct StoreT4Chain {
   static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile& t, const TileOffsets&,
                                              cpx (&v)[R]) {
     constexpr int TPT = L / R;
-    const int64_t b2 = x.b / (p.d0 * p.d1);
+    const int64_t b2 = udiv(x.b, p.d0 * p.d1);
     real* out = static_cast<real*>(p.out) + b2 * p.k_out_line;
     const bool dst = (p.flags & F_DST) != 0;
     const int h = p.cpb / 2;
@@ -1202,8 +1202,8 @@ template <bool kMirror>
 __device__ __forceinline__ int64_t tile_batch(const AxisParams& p, int c) {
   if constexpr (kMirror) {
     const int64_t M = p.d0 * p.d1;
-    const int64_t per_line = M / p.cpb;  // CTAs per line
-    const int64_t line = int64_t(blockIdx.x) / per_line, q = int64_t(blockIdx.x) % per_line;
+    const int64_t per_line = udiv(M, p.cpb);  // CTAs per line
+    const int64_t line = udiv(int64_t(blockIdx.x), per_line), q = int64_t(blockIdx.x) - line * per_line;
     const int h = p.cpb / 2;
     const int64_t i = q * h + (c < h ? c : c - h);
     return line * M + (c < h ? i : M - 1 - i);
@@ -1258,7 +1258,7 @@ __global__ void __launch_bounds__(512, MinBlocks<R>::value) axis_pass_kernel(con
   x.active = x.b < p.nbatch;
   x.oin = to.in_off[x.c];
   x.oout = to.out_off[x.c];
-  x.b0 = x.b % p.d0;
+  x.b0 = umod(x.b, p.d0);
 
   cpx v[R];
   LoadOp::template run<L, R>(p, x, t, v);

@@ -142,6 +142,16 @@ __device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.lau
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // --------------------------------------------------------------- misc utils
+// Quotient and remainder of non-negative 64-bit values, in 32-bit
+// arithmetic when both fit in 31 bits (every batch index and extent of the
+// plans in practice; the 64-bit sequences are several times longer).
+__device__ __forceinline__ int64_t udiv(int64_t a, int64_t b) {
+  return ((a | b) >> 31) == 0 ? int64_t(uint32_t(a) / uint32_t(b)) : a / b;
+}
+__device__ __forceinline__ int64_t umod(int64_t a, int64_t b) {
+  return ((a | b) >> 31) == 0 ? int64_t(uint32_t(a) % uint32_t(b)) : a % b;
+}
+
 __device__ __forceinline__ int pad16(int p) { return p + (p >> 4); }
 __host__ __device__ constexpr int padded_len(int L) { return L + (L >> 4); }
 

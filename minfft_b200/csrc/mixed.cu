@@ -221,7 +221,7 @@ __device__ __forceinline__ void big_pass(const Params& mp, const cpx* src, cpx* 
     x.j = j;
     x.b = base + c;
     x.active = x.b < NJ;
-    x.b0 = x.b % p.d0;
+    x.b0 = umod(x.b, p.d0);
     x.oin = offs[c];
     x.oout = offs[CPB + c];
     cpx v[R];

@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(512, MinBlocks<R>::value) axis_pipe_kernel(con
   // first transform and count of a tile
   auto tile_span = [&](int64_t t, int64_t& b_first, int& nvalid) {
     if (p.colmode) {
-      const int64_t blk = t / p.gpb, g = t - blk * p.gpb;
+      const int64_t blk = udiv(t, p.gpb), g = t - blk * p.gpb;
       const int64_t start = g * cpb;
       b_first = blk * p.d0 + start;
       nvalid = int((p.d0 - start) < cpb ? (p.d0 - start) : cpb);
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(512, MinBlocks<R>::value) axis_pipe_kernel(con
     x.j = j;
     x.b = bf + c;
     x.active = c < nv;
-    x.b0 = x.b % p.d0;
+    x.b0 = umod(x.b, p.d0);
     x.oin = 0;
     x.oout = to.out_off[c];
     cpx v[R];

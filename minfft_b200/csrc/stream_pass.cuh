@@ -141,10 +141,10 @@ __global__ void __launch_bounds__(stream_cols() * (L / R), 1)
 
   // tile t -> first column, block indices
   auto tile_pos = [&](int64_t t, int64_t& col0, int64_t& b1, int64_t& b2) {
-    const int64_t rest = t / gpd;
+    const int64_t rest = udiv(t, gpd);
     col0 = (t - rest * gpd) * W;
-    b1 = rest % p.d1;
-    b2 = rest / p.d1;
+    b2 = udiv(rest, p.d1);
+    b1 = rest - b2 * p.d1;
   };
 
   // start the copy of tile t into stage s
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(512, 1) stream_rows_kernel(const AxisParams p)
     x.c = tid / TPT;
     x.b = b0t + x.c;
     x.active = x.c < nv;
-    x.b0 = x.b % p.d0;
+    x.b0 = umod(x.b, p.d0);
     x.oin = int64_t(x.c) * (p.row_pitch / esz);
     x.oout = offs[cpb + x.c];
     // the kind's load stage, on the rows in the stage

@@ -230,7 +230,7 @@ __device__ __forceinline__ void tile_offsets(const AxisParams& p, int64_t tile, 
     batch_offsets(p, b < p.nbatch ? b : 0, b0, oi, oo);
     offs[tid] = oi;
     offs[TB + tid] = oo;
-    gq[tid] = p.st_ns > 1 ? ((b0 / p.st_div) & (p.st_ns - 1)) << p.st_shift : 0;
+    gq[tid] = p.st_ns > 1 ? (udiv(b0, p.st_div) & (p.st_ns - 1)) << p.st_shift : 0;
   }
 }
 
@@ -720,10 +720,10 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
   const uint32_t tmem = *tslot;
 
   auto tile_pos = [&](int64_t t, int64_t& c0, int64_t& b1, int64_t& b2) {
-    const int64_t rest = t / gpd;
+    const int64_t rest = udiv(t, gpd);
     c0 = (t - rest * gpd) * W;
-    b1 = rest % p.d1;
-    b2 = rest / p.d1;
+    b2 = udiv(rest, p.d1);
+    b1 = rest - b2 * p.d1;
   };
   // tile element (transform cc, point n) -> complex index in the stage
   auto pos_in = [&](int cc, int n) { return ROWS ? (n >> 7) * (W * 128) + cc * 128 + (n & 127) : n * W + cc; };
@@ -802,7 +802,7 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
     if (twid) {
       // pre-twiddle of a later pass of a Stockham chain: element n = 16 n1 + d
       // times w_Lt^(n * gq) = w^(d*gq) * (w^(16*gq))^n1
-      const int64_t gq = ((col / p.st_div) & (p.st_ns - 1)) << p.st_shift;
+      const int64_t gq = (udiv(col, p.st_div) & (p.st_ns - 1)) << p.st_shift;
       const cpx base = stockham_root(p, int64_t(d) * gq);
       const cpx d1 = stockham_root(p, 16 * gq);
       const cpx d2 = cmul(d1, d1);
