@@ -568,9 +568,8 @@ struct Planner {
 
   // Form of the tensor-core pass: the streamed form (tc_stream_kernel) by
   // default, the one-tile form with MINFFT_B200_TC_FORM=tile; stages of the
-  // streamed form from MINFFT_B200_TC_STAGES (2 .. 6; default 2 for FP16,
-  // which then fits two CTAs per SM, and 3 for BF16, whose larger operands
-  // allow one).
+  // streamed form from MINFFT_B200_TC_STAGES (2 .. 6; default 2, which fits
+  // four CTAs per SM in FP16 and three in BF16).
   static bool tc_stream_default() {
     static const bool on = [] {
       const char* e = getenv("MINFFT_B200_TC_FORM");
@@ -578,13 +577,13 @@ struct Planner {
     }();
     return on;
   }
-  static int tc_stream_stages(int fmt) {
+  static int tc_stream_stages(int) {
     static const int n = [] {
       const char* e = getenv("MINFFT_B200_TC_STAGES");
       const int v = e ? atoi(e) : 0;
       return v <= 0 ? 0 : (v < 2 ? 2 : (v > 6 ? 6 : v));
     }();
-    return n ? n : (fmt == mb::TC_F16 ? 2 : 3);
+    return n ? n : 2;
   }
 
   // Normalised layout of the streamed tensor-core pass: b0 indexes the
@@ -648,7 +647,7 @@ struct Planner {
     ap.lp = 0;
     ln.block = unsigned(mb::kTcStreamThreads);
     // resident CTAs per SM, counted here from registers, shared memory,
-    // threads and the 128 tensor-memory columns a CTA allocates (the
+    // threads and the tensor-memory columns a CTA allocates (the
     // occupancy calculator reports one CTA per SM for kernels that allocate
     // tensor memory)
     int occ = 1;
@@ -662,7 +661,7 @@ struct Planner {
         const int regs_cta = warps * ((fa.numRegs * 32 + 255) / 256 * 256);
         const size_t smem_cta = ln.smem + fa.sharedSizeBytes + 1024;  // + the per-CTA reservation
         occ = std::min({regs_sm / std::max(regs_cta, 1), int(size_t(smem_sm) / smem_cta), 2048 / int(ln.block),
-                        512 / 128});
+                        512 / mb::kTcStreamTmemCols});
         occ = std::max(occ, 1);
       } else {
         cudaGetLastError();
@@ -1972,7 +1971,8 @@ bool tc_stream_map(CUtensorMap* m, const Launch& ln, const AxisParams& ap) {
   const cuuint64_t strides[3] = {cuuint64_t(s1), cuuint64_t(st1), cuuint64_t(st2)};
   for (int i = 0; i < 3; ++i)
     if (strides[i] >= (uint64_t(1) << 40)) return false;
-  const cuuint32_t box[4] = {cuuint32_t(rows ? 256 : 32), cuuint32_t(rows ? 16 : 128), 1, 1};
+  const cuuint32_t box[4] = {cuuint32_t(rows ? 256 : 2 * mb::kTcStreamTile), cuuint32_t(rows ? mb::kTcStreamTile : 128),
+                              1, 1};
   const cuuint32_t es[4] = {1, 1, 1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(ap.in), dims, strides, box, es,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,

@@ -529,29 +529,35 @@ __global__ void __launch_bounds__(16 * TB, TB == 8 ? 4 : 2) tc256_kernel(const A
 
 // ===================================================== streamed TC pass
 // The same two radix-16 contractions, on the tile pipeline of the streamed
-// column pass (stream_pass.cuh): persistent CTAs, tiles of 16 transforms of
-// 256 points copied into S shared-memory stages by tensor copies (or
-// cp.async where the strides do not allow them), an mbarrier per stage.
+// column pass (stream_pass.cuh): persistent CTAs of 128 threads (one UMMA
+// group of 128 rows, four warps), tiles of 8 transforms of 256 points copied
+// into S shared-memory stages by tensor copies (or cp.async where the
+// strides do not allow them), an mbarrier per stage.  Small CTAs let four of
+// them share an SM in FP16 (three in BF16), so that while one waits for its
+// matrix operations or its barriers the others issue: with 256-thread CTAs
+// of two groups, two per SM, the pass ran 10-20% slower.
 //
 // Thread t owns row t of the contraction: in stage 1 the sub-DFT (c, n2) --
 // inputs x[16 n1 + n2], n1 = 0..15 -- and in stage 2 the sub-DFT (c, k1) --
 // inputs y1[16 k1 + n2] after the twiddles, n2 = 0..15 -- with c the
 // transform of the tile and the digit d = n2 (stage 1) or k1 (stage 2):
-// column tiles c = t % 16, d = t / 16; row tiles d = t % 16, c = t / 16, so
-// that in both the 16 threads of a half warp read 128 contiguous bytes of
-// the tile.  Each row is scaled by its own power of two (largest component
-// into [2^8, 2^9)), split into NT 16-bit terms and written as row t of the
-// K-major A operand of its group of 128 rows; thread 0 issues the MMAs of
-// both groups (corrections into one accumulator, the leading product into
-// another) and commits them to an mbarrier; every thread reads its row of
-// both accumulators with one tcgen05.ld each, adds them and unscales.
+// column tiles c = t % 8, d = t / 8; row tiles d = t % 16, c = t / 16, so
+// that a warp reads contiguous runs of the tile.  Each row is scaled by its
+// own power of two (largest component into [2^8, 2^9)), split into NT
+// 16-bit terms and written as row t of the K-major A operand; thread 0
+// issues the MMAs (corrections into one accumulator, the leading product
+// into another) and commits them to an mbarrier; every thread reads its row
+// of both accumulators with one tcgen05.ld each, adds them and unscales.
 //
 // Between the stages the twiddled values go back into the stage, which then
 // holds y1 in a layout chosen per tile kind so that the writes (lanes over
 // n2) and the reads (lanes over k1) are both conflict-free: column tiles
-// (16 k1 + n2) * 16 + c, row tiles c * 256 + 16 k1 + (n2 ^ k1).
-constexpr int kTcsW = 16;     // transforms per tile
-constexpr int kTcsNT = 256;   // threads
+// (16 k1 + (n2 ^ (k1 & 1))) * 8 + c (a warp's four k1 rows of 64 bytes then
+// fall on both halves of the banks), row tiles c * 256 + 16 k1 + (n2 ^ k1).
+constexpr int kTcsW = kTcStreamTile;     // transforms per tile
+constexpr int kTcsNT = kTcStreamThreads; // threads
+constexpr int kTcsG = kTcsNT / 128;      // UMMA groups of 128 rows
+static_assert(kTcsW * 16 == kTcsNT, "one contraction row per thread");
 constexpr int kTcsStages = 2;
 
 template <int FMT>
@@ -560,9 +566,10 @@ struct TcsLayout {
   static constexpr int bar_bytes = 128;                  // mbarriers, TMEM slot, flag
   static constexpr int b_off = bar_bytes;                // B operands: NT x 2 KB
   static constexpr int tw_off = b_off + NT * kBBytes;    // w_256^m, m < 256 (2 KB)
-  static constexpr int a_off = tw_off + kL * 8;          // A operands: 2 groups x NT x 8 KB
-  static constexpr int st_off = a_off + 2 * NT * kOpBytes;
-  static constexpr int tmem_cols = 128;                  // 2 groups x (leading, correction) x 32
+  static constexpr int a_off = tw_off + kL * 8;          // A operands: groups x NT x 8 KB
+  static constexpr int st_off = a_off + kTcsG * NT * kOpBytes;
+  static constexpr int tmem_cols = 64 * kTcsG;           // groups x (leading, correction) x 32
+  static_assert(tmem_cols == kTcStreamTmemCols, "tensor-memory columns");
 };
 
 __host__ __device__ inline int tcs_stage_bytes() { return (kTcsW * (kL + 1) * 8 + 127) / 128 * 128; }
@@ -611,7 +618,7 @@ __device__ __forceinline__ void tcs_write_a(unsigned char* aop, int g, int row, 
     }
 #pragma unroll
     for (int z = 0; z < NT; ++z)
-      *reinterpret_cast<uint4*>(aop + (z * 2 + g) * kOpBytes + tc_operand_offset(row, kb * 8)) =
+      *reinterpret_cast<uint4*>(aop + (z * kTcsG + g) * kOpBytes + tc_operand_offset(row, kb * 8)) =
           make_uint4(w[z][0], w[z][1], w[z][2], w[z][3]);
   }
 }
@@ -624,7 +631,7 @@ __device__ __forceinline__ void tcs_issue_mma(uint32_t aop_a, uint32_t bop_a, ui
   constexpr uint32_t idesc = instr_desc<FMT>();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-  for (int g = 0; g < 2; ++g) {
+  for (int g = 0; g < kTcsG; ++g) {
     uint32_t acc = 0;
 #pragma unroll
     for (int sum = NT - 1; sum >= 1; --sum)
@@ -633,7 +640,7 @@ __device__ __forceinline__ void tcs_issue_mma(uint32_t aop_a, uint32_t bop_a, ui
         const int j = sum - i;
 #pragma unroll
         for (int kh = 0; kh < 2; ++kh) {
-          const uint64_t ad = smem_desc(aop_a + (i * 2 + g) * kOpBytes + kh * 256);
+          const uint64_t ad = smem_desc(aop_a + (i * kTcsG + g) * kOpBytes + kh * 256);
           const uint64_t bd = smem_desc(bop_a + j * kBBytes + kh * 256);
           mma_f16(tmem + uint32_t(64 * g + 32), ad, bd, idesc, acc);
           acc = 1;
@@ -641,7 +648,7 @@ __device__ __forceinline__ void tcs_issue_mma(uint32_t aop_a, uint32_t bop_a, ui
       }
 #pragma unroll
     for (int kh = 0; kh < 2; ++kh) {
-      const uint64_t ad = smem_desc(aop_a + g * kOpBytes + kh * 256);
+      const uint64_t ad = smem_desc(aop_a + g * kOpBytes + kh * 256);  // term 0 of group g
       const uint64_t bd = smem_desc(bop_a + kh * 256);
       mma_f16(tmem + uint32_t(64 * g), ad, bd, idesc, kh);
     }
@@ -664,7 +671,7 @@ __device__ __forceinline__ void tcs_read_d(uint32_t tmem, int warp, float (&re)[
 }
 
 template <int FMT, bool ROWS>
-__global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kernel(const AxisParams p, const TcParams q,
+__global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 4 : 3) tc_stream_kernel(const AxisParams p, const TcParams q,
                                                               const __grid_constant__ CUtensorMap tmap) {
   using Lay = TcsLayout<FMT>;
   constexpr int NT = Lay::NT;
@@ -679,8 +686,8 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
   unsigned char* stages = sm + Lay::st_off;
   const int S = p.cpb;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int c = ROWS ? tid / 16 : tid % 16;  // transform of the tile
-  const int d = ROWS ? tid % 16 : tid / 16;  // digit: n2 in stage 1, k1 in stage 2
+  const int c = ROWS ? tid / 16 : tid % kTcsW;  // transform of the tile
+  const int d = ROWS ? tid % 16 : tid / kTcsW;  // digit: n2 in stage 1, k1 in stage 2
   const int g = tid >> 7, row = tid & 127;   // UMMA group and row
   const bool tma = (p.flags & F_STREAM_TMA) != 0;
   const uint32_t bar0 = static_cast<uint32_t>(__cvta_generic_to_shared(bars));
@@ -711,7 +718,7 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
     const uint4* src = reinterpret_cast<const uint4*>(q.bmat);
     uint4* dst = reinterpret_cast<uint4*>(bop);
     for (int i = tid; i < NT * kBBytes / 16; i += kTcsNT) dst[i] = src[i];
-    tws[tid] = ldg(p.tw + tid);  // the twiddles between the stages, read from shared memory
+    for (int i = tid; i < kL; i += kTcsNT) tws[i] = ldg(p.tw + i);  // the twiddles between the stages
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -739,8 +746,8 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(W * kL * 8) : "memory");
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          // column tiles: box (32 reals = 16 transforms, 128 points); row
-          // tiles: box (256 reals = 128 points, 16 transforms)
+          // column tiles: box (2W reals = W transforms, 128 points); row
+          // tiles: box (256 reals = 128 points, W transforms)
           const int x0 = ROWS ? 256 * h : int(2 * c0);
           const int x1 = ROWS ? int(c0) : 128 * h;
           asm volatile(
@@ -848,7 +855,7 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
     for (int k1 = 0; k1 < 16; ++k1) {
       const cpx w = tws[d * k1];
       const cpx y = cmul(cmk(re[k1] * inv, im[k1] * inv), w);
-      const int idx = ROWS ? c * kL + 16 * k1 + (d ^ k1) : (16 * k1 + d) * W + c;
+      const int idx = ROWS ? c * kL + 16 * k1 + (d ^ k1) : (16 * k1 + (d ^ (k1 & 1))) * W + c;
       tile[idx] = y;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -857,7 +864,7 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 2 : 1) tc_stream_kerne
     // ---- stage 2: row (c, k1 = d), inputs y1[16 d + n2], n2 = 0..15
 #pragma unroll
     for (int n2 = 0; n2 < 16; ++n2) {
-      const int idx = ROWS ? c * kL + 16 * d + (n2 ^ d) : (16 * d + n2) * W + c;
+      const int idx = ROWS ? c * kL + 16 * d + (n2 ^ d) : (16 * d + (n2 ^ (d & 1))) * W + c;
       const cpx u = tile[idx];
       re[n2] = u.x;
       im[n2] = u.y;

@@ -38,16 +38,17 @@ constexpr int kTcLength = 256;
 const void* tc_kernel(int fmt, int tb);
 size_t tc_smem(int fmt, int tb);
 
-// The streamed form (persistent CTAs of 256 threads, tiles of 16 transforms
+// The streamed form (persistent CTAs of 128 threads, tiles of 8 transforms
 // fed through `stages` shared-memory stages by tensor copies or cp.async;
 // arguments (AxisParams with cpb = stages, TcParams, CUtensorMap)): column
-// tiles (16 adjacent transforms, unit stride between them) or row tiles
-// (16 transforms of contiguous points).  nullptr in the double library.
+// tiles (8 adjacent transforms, unit stride between them) or row tiles
+// (8 transforms of contiguous points).  nullptr in the double library.
 const void* tc_stream_kernel_fn(int fmt, bool rows);
 size_t tc_stream_smem(int fmt, int stages);
 int tc_stream_stage_bytes();
-constexpr int kTcStreamThreads = 256;
-constexpr int kTcStreamTile = 16;
+constexpr int kTcStreamThreads = 128;
+constexpr int kTcStreamTile = 8;
+constexpr int kTcStreamTmemCols = 64;  // a leading and a correction accumulator of 32 columns
 inline int tc_threads(int tb) { return 16 * tb; }
 // Tensor-memory columns a CTA allocates: per 8 transforms, a leading and a
 // correction accumulator of 32 FP32 columns each.
