@@ -120,10 +120,10 @@ __global__ void __launch_bounds__(8 * (L / R), 1) dctq_row_fwd(const DctqParams 
         StoreDCT2::emit(st, 1, k, N, dst, cconj(za[i]), w128(8));
       } else {
         cpx xa, xb;
-        unpack_pair(za[i], zb[i], rft_root<R>(b2, i), xa, xb);
+        unpack_pair2(za[i], zb[i], rft_root<R>(b2, i), xa, xb);
         const cpx e = t23_root<R>(b1, i);
-        StoreDCT2::emit(st, 1, k, N, dst, xa, e);
-        StoreDCT2::emit(st, 1, L - k, N, dst, xb, t23_mirror(e));
+        StoreDCT2::emit2(st, 1, k, N, dst, xa, e);
+        StoreDCT2::emit2(st, 1, L - k, N, dst, xb, t23_mirror(e));
       }
     }
   }
@@ -218,9 +218,9 @@ __global__ void __launch_bounds__(512, 1) dctq_col_fwd(const DctqParams q) {
       StoreDCT2::emit(o, N, int(k), int(Nr), dst, cconj(za), ldg(q.t23_c + k));
     } else {
       cpx xa, xb;
-      unpack_pair(za, zb, ldg(q.rft_c + k), xa, xb);
-      StoreDCT2::emit(o, N, int(k), int(Nr), dst, xa, ldg(q.t23_c + k));
-      StoreDCT2::emit(o, N, int(Lc - k), int(Nr), dst, xb, ldg(q.t23_c + (Lc - k)));
+      unpack_pair2(za, zb, ldg(q.rft_c + k), xa, xb);
+      StoreDCT2::emit2(o, N, int(k), int(Nr), dst, xa, ldg(q.t23_c + k));
+      StoreDCT2::emit2(o, N, int(Lc - k), int(Nr), dst, xb, ldg(q.t23_c + (Lc - k)));
     }
   }
 }

@@ -189,9 +189,9 @@ struct Op_dct2_post {
       StoreDCT2::emit(out, p.out_sn, k, N, dst, cconj(za), root1(p, k));
     } else {
       cpx xa, xb;
-      unpack_pair(za, in[(L - k) * p.in_sn], root2(p, k), xa, xb);
-      StoreDCT2::emit(out, p.out_sn, k, N, dst, xa, root1(p, k));
-      StoreDCT2::emit(out, p.out_sn, int(L) - k, N, dst, xb, root1(p, L - k));
+      unpack_pair2(za, in[(L - k) * p.in_sn], root2(p, k), xa, xb);
+      StoreDCT2::emit2(out, p.out_sn, k, N, dst, xa, root1(p, k));
+      StoreDCT2::emit2(out, p.out_sn, int(L) - k, N, dst, xb, root1(p, L - k));
     }
   }
 };

@@ -522,9 +522,9 @@ __device__ __forceinline__ void big_post_pair(const Params& mp, const Item& it, 
     StoreDCT2::emit(out, 1, int(k), int(N), dst, cconj(za), ldg(t23 + k));
   } else {
     cpx xa, xb;
-    unpack_pair(za, zb, ldg(rft + k), xa, xb);
-    StoreDCT2::emit(out, 1, int(k), int(N), dst, xa, ldg(t23 + k));
-    StoreDCT2::emit(out, 1, int(L - k), int(N), dst, xb, ldg(t23 + (L - k)));
+    unpack_pair2(za, zb, ldg(rft + k), xa, xb);
+    StoreDCT2::emit2(out, 1, int(k), int(N), dst, xa, ldg(t23 + k));
+    StoreDCT2::emit2(out, 1, int(L - k), int(N), dst, xb, ldg(t23 + (L - k)));
   }
 }
 

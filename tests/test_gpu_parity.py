@@ -132,6 +132,20 @@ def test_parity_long_1d(n, single):
 
 
 @pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
+@pytest.mark.parametrize("n", [1 << 21, 1 << 22])
+def test_parity_three_pass_chains(n, single):
+    """The CUDA-core chains cap their passes over HBM at 1024 points, so
+    2^21 .. 2^24-point axes take three passes (for the real kinds, of their
+    half-length complex DFT): every transform kind against the oracle."""
+    rng = np.random.default_rng(n + 3)
+    dims = (n,)
+    for op in OPS:
+        x = make_input(op, dims, rng, single)
+        err = rel_l2(gpu_apply(op, x, dims, single), expected(op, x, dims))
+        assert err <= tolerance(single, dims), (op, n, err)
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["f64", "f32"])
 @pytest.mark.parametrize("dims", [(8192, 4), (4, 8192), (2, 16384), (16384, 2), (8, 8, 8192)],
                          ids=lambda d: "x".join(map(str, d)))
 def test_parity_long_axes_multid(dims, single):
