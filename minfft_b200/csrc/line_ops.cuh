@@ -33,10 +33,10 @@ struct ItemIdx {
 
 __device__ __forceinline__ ItemIdx split_item(int64_t e, int64_t inner, int64_t K) {
   ItemIdx r;
-  r.i = e % inner;
-  const int64_t q = e / inner;
-  r.n = q % K;
-  r.o = q / K;
+  const int64_t q = udiv(e, inner);
+  r.i = e - q * inner;
+  r.o = udiv(q, K);
+  r.n = q - r.o * K;
   return r;
 }
 
