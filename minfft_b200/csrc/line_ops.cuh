@@ -1,8 +1,12 @@
 // Element-wise pre- and post-processing steps of real-data transforms whose
 // half-length complex DFT runs as several HBM passes, and the length-1 axis
 // steps, as device functions: Op::count(p) work items, Op::item(p, e) does
-// item e.  Used by the line kernels (line_kernels.cu) and by the mixed-batch
-// kernel (mixed.cu).
+// item e.  The steps of the real kinds also come as Op::load(p, e), which
+// reads everything item e needs (data and roots) into an Op::In, and
+// Op::finish(p, e, in), which computes and stores: a CTA that walks a line
+// alone (the mixed-batch kernel) then issues the loads of several items
+// before any of their stores.  Used by the line kernels (line_kernels.cu)
+// and by the mixed-batch kernel (mixed.cu).
 //
 // Data layout: a batch of outer x inner lines along one axis; element n of
 // line (o, i) of the input sits at o*in_so + n*in_sn + i, of the output at
@@ -46,16 +50,26 @@ struct Op_dct2_pre {
     const int64_t L = p.L;
     return p.outer * p.inner * L;
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+  struct In {
+    real a, b;
+  };
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
     const int64_t L = p.L, N = 2 * L;
-    const real sg = (p.flags & F_DST) ? real(-1) : real(1);
     const ItemIdx it = split_item(e, p.inner, L);
     const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
     const int64_t i0 = 2 * it.n, i1 = 2 * it.n + 1;
-    const real a = i0 < L ? in[(2 * i0) * p.in_sn] : sg * in[(2 * N - 1 - 2 * i0) * p.in_sn];
-    const real b = i1 < L ? in[(2 * i1) * p.in_sn] : sg * in[(2 * N - 1 - 2 * i1) * p.in_sn];
-    static_cast<cpx*>(p.out)[it.o * p.out_so + it.n * p.out_sn + it.i] = cmk(a, b);
+    return In{i0 < L ? in[(2 * i0) * p.in_sn] : in[(2 * N - 1 - 2 * i0) * p.in_sn],
+              i1 < L ? in[(2 * i1) * p.in_sn] : in[(2 * N - 1 - 2 * i1) * p.in_sn]};
   }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    const int64_t L = p.L;
+    const real sg = (p.flags & F_DST) ? real(-1) : real(1);
+    const ItemIdx it = split_item(e, p.inner, L);
+    const int64_t i0 = 2 * it.n, i1 = 2 * it.n + 1;
+    static_cast<cpx*>(p.out)[it.o * p.out_so + it.n * p.out_sn + it.i] =
+        cmk(i0 < L ? v.a : sg * v.a, i1 < L ? v.b : sg * v.b);
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
 };
 
 // type-4 pre-rotation (see LoadT4)
@@ -64,23 +78,29 @@ struct Op_t4_pre {
     const int64_t L = p.L;
     return p.outer * p.inner * L;
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+  struct In {
+    real a, b;
+    cpx w;
+  };
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
     const int64_t L = p.L, N = 2 * L;
-    const bool dst = (p.flags & F_DST) != 0;
     const ItemIdx it = split_item(e, p.inner, L);
     const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
-    const real a = in[(2 * it.n) * p.in_sn];
-    const real b = in[(N - 1 - 2 * it.n) * p.in_sn];
-    const cpx w = root1(p, it.n);
+    return In{in[(2 * it.n) * p.in_sn], in[(N - 1 - 2 * it.n) * p.in_sn], root1(p, it.n)};
+  }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& x) {
+    const bool dst = (p.flags & F_DST) != 0;
+    const ItemIdx it = split_item(e, p.inner, p.L);
     cpx v;
     if (!dst) {
-      v = cmul(w, cmk(a, b));
+      v = cmul(x.w, cmk(x.a, x.b));
     } else {
-      const cpx q = cmul(w, cmk(a, -b));
+      const cpx q = cmul(x.w, cmk(x.a, -x.b));
       v = cmk(-q.x, -q.y);
     }
     static_cast<cpx*>(p.out)[it.o * p.out_so + it.n * p.out_sn + it.i] = v;
   }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
 };
 
 // inverse-real-DFT packing, conjugated (see LoadC2R); in: L+1 spectrum values
@@ -89,24 +109,33 @@ struct Op_c2r_pack {
     const int64_t L = p.L, K = L / 2 + 1;
     return p.outer * p.inner * K;
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+  struct In {
+    cpx z0, z1, f;
+  };
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
     const int64_t L = p.L, K = L / 2 + 1;
     const ItemIdx it = split_item(e, p.inner, K);
     const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
+    const int64_t k = it.n;
+    return In{in[k * p.in_sn], in[(L - k) * p.in_sn], (k != 0 && 2 * k != L) ? root2(p, k) : czero()};
+  }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const ItemIdx it = split_item(e, p.inner, K);
     cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
     const int64_t k = it.n;
-    const cpx z0 = in[k * p.in_sn], z1 = in[(L - k) * p.in_sn];
     if (k == 0) {
-      out[0] = cmk(z0.x + z1.x, -(z0.x - z1.x));
+      out[0] = cmk(v.z0.x + v.z1.x, -(v.z0.x - v.z1.x));
     } else if (2 * k == L) {
-      out[k * p.out_sn] = cmk(2 * z0.x, 2 * z0.y);
+      out[k * p.out_sn] = cmk(2 * v.z0.x, 2 * v.z0.y);
     } else {
       cpx ta, tb;
-      pack_pair(z0, z1, root2(p, k), ta, tb);
+      pack_pair(v.z0, v.z1, v.f, ta, tb);
       out[k * p.out_sn] = cconj(ta);
       out[(L - k) * p.out_sn] = cconj(tb);
     }
   }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
 };
 
 // type-3 pre-rotation + packing, conjugated (see LoadDCT3)
@@ -115,27 +144,39 @@ struct Op_dct3_pack {
     const int64_t L = p.L, K = L / 2 + 1;
     return p.outer * p.inner * K;
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+  struct In {
+    cpx z0, z1, f;
+  };
+  // the reads and the pre-rotation of both values of the pair
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
     const int64_t L = p.L, K = L / 2 + 1;
     const bool dst = (p.flags & F_DST) != 0;
     const ItemIdx it = split_item(e, p.inner, K);
     const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
-    cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
     const int k = int(it.n);
     auto rd = [&](int i) { return in[int64_t(i) * p.in_sn]; };
-    const cpx z0 = LoadDCT3::zval_w(rd, k, int(L), dst, [&](int n) { return root1(p, n); });
-    const cpx z1 = LoadDCT3::zval_w(rd, int(L) - k, int(L), dst, [&](int n) { return root1(p, n); });
+    return In{LoadDCT3::zval_w(rd, k, int(L), dst, [&](int n) { return root1(p, n); }),
+              LoadDCT3::zval_w(rd, int(L) - k, int(L), dst, [&](int n) { return root1(p, n); }),
+              (k != 0 && 2 * k != L) ? root2(p, k) : czero()};
+  }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const ItemIdx it = split_item(e, p.inner, K);
+    cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
+    const int k = int(it.n);
+    const cpx z0 = v.z0, z1 = v.z1;
     if (k == 0) {
       out[0] = cmk(z0.x + z1.x, -(z0.x - z1.x));
     } else if (2 * k == L) {
       out[k * p.out_sn] = cmk(2 * z0.x, 2 * z0.y);
     } else {
       cpx ta, tb;
-      pack_pair(z0, z1, root2(p, k), ta, tb);
+      pack_pair(z0, z1, v.f, ta, tb);
       out[k * p.out_sn] = cconj(ta);
       out[(L - k) * p.out_sn] = cconj(tb);
     }
   }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
 };
 
 // real-DFT unpacking (see StoreR2C); out: L+1 spectrum values
@@ -144,13 +185,23 @@ struct Op_r2c_unpack {
     const int64_t L = p.L, K = L / 2 + 1;
     return p.outer * p.inner * K;
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+  struct In {
+    cpx za, zb, f;
+  };
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
     const int64_t L = p.L, K = L / 2 + 1;
     const ItemIdx it = split_item(e, p.inner, K);
     const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
+    const int64_t k = it.n;
+    const bool pair = k != 0 && 2 * k != L;
+    return In{in[k * p.in_sn], pair ? in[(L - k) * p.in_sn] : czero(), pair ? root1(p, k) : czero()};
+  }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const ItemIdx it = split_item(e, p.inner, K);
     cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
     const int64_t k = it.n;
-    const cpx za = in[k * p.in_sn];
+    const cpx za = v.za;
     if (k == 0) {
       out[0] = cmk(za.x + za.y, real(0));
       out[L * p.out_sn] = cmk(za.x - za.y, real(0));
@@ -158,11 +209,12 @@ struct Op_r2c_unpack {
       out[k * p.out_sn] = cconj(za);
     } else {
       cpx xa, xb;
-      unpack_pair(za, in[(L - k) * p.in_sn], root1(p, k), xa, xb);
+      unpack_pair(za, v.zb, v.f, xa, xb);
       out[k * p.out_sn] = xa;
       out[(L - k) * p.out_sn] = xb;
     }
   }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
 };
 
 // type-2 unpacking + post-rotation (see StoreDCT2)
@@ -171,29 +223,41 @@ struct Op_dct2_post {
     const int64_t L = p.L, K = L / 2 + 1;
     return p.outer * p.inner * K;
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+  struct In {
+    cpx za, zb, f, ea, eb;
+  };
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+    const int64_t L = p.L, K = L / 2 + 1;
+    const ItemIdx it = split_item(e, p.inner, K);
+    const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
+    const int64_t k = it.n;
+    const bool pair = k != 0 && 2 * k != L;
+    return In{in[k * p.in_sn], pair ? in[(L - k) * p.in_sn] : czero(), pair ? root2(p, k) : czero(),
+              k != 0 ? root1(p, k) : czero(), pair ? root1(p, L - k) : czero()};
+  }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
     const int64_t L = p.L, K = L / 2 + 1;
     const int N = int(2 * L);
     const bool dst = (p.flags & F_DST) != 0;
     const real r2 = real(1.414213562373095048801688724209698079);
     const ItemIdx it = split_item(e, p.inner, K);
-    const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
     real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
     const int k = int(it.n);
-    const cpx za = in[k * p.in_sn];
+    const cpx za = v.za;
     if (k == 0) {
       const real v0 = za.x + za.y, vl = za.x - za.y;
       out[int64_t(dst ? N - 1 : 0) * p.out_sn] = 2 * v0;
       out[int64_t(dst ? L - 1 : L) * p.out_sn] = r2 * vl;
     } else if (2 * k == L) {
-      StoreDCT2::emit(out, p.out_sn, k, N, dst, cconj(za), root1(p, k));
+      StoreDCT2::emit(out, p.out_sn, k, N, dst, cconj(za), v.ea);
     } else {
       cpx xa, xb;
-      unpack_pair2(za, in[(L - k) * p.in_sn], root2(p, k), xa, xb);
-      StoreDCT2::emit2(out, p.out_sn, k, N, dst, xa, root1(p, k));
-      StoreDCT2::emit2(out, p.out_sn, int(L) - k, N, dst, xb, root1(p, L - k));
+      unpack_pair2(za, v.zb, v.f, xa, xb);
+      StoreDCT2::emit2(out, p.out_sn, k, N, dst, xa, v.ea);
+      StoreDCT2::emit2(out, p.out_sn, int(L) - k, N, dst, xb, v.eb);
     }
   }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
 };
 
 // type-3 de-interleave of the conjugated forward result (see StoreDCT3)
@@ -202,11 +266,19 @@ struct Op_dct3_post {
     const int64_t L = p.L;
     return p.outer * p.inner * L;
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+  struct In {
+    cpx w;
+  };
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+    const ItemIdx it = split_item(e, p.inner, p.L);
+    return In{static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i]};
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
     const int64_t L = p.L, N = 2 * L;
     const bool dst = (p.flags & F_DST) != 0;
     const ItemIdx it = split_item(e, p.inner, L);
-    const cpx w = cconj(static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i]);
+    const cpx w = cconj(v.w);
     real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
     const int64_t i0 = 2 * it.n, i1 = 2 * it.n + 1;
     const real a = (dst && i0 >= L) ? -w.x : w.x;
@@ -222,15 +294,25 @@ struct Op_t4_post {
     const int64_t L = p.L;
     return p.outer * p.inner * L;
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+  struct In {
+    cpx T, ga, gb;
+  };
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+    const int64_t N = 2 * p.L;
+    const ItemIdx it = split_item(e, p.inner, p.L);
+    const int64_t m = it.n;
+    return In{static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i], root2(p, 2 * m),
+              root2(p, N - 1 - 2 * m)};
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
     const int64_t L = p.L, N = 2 * L;
     const bool dst = (p.flags & F_DST) != 0;
     const ItemIdx it = split_item(e, p.inner, L);
-    const cpx T = static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i];
     real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
     const int64_t m = it.n;
-    const cpx a = cmul(root2(p, 2 * m), T);
-    const cpx b = cmul(root2(p, N - 1 - 2 * m), cconj(T));
+    const cpx a = cmul(v.ga, v.T);
+    const cpx b = cmul(v.gb, cconj(v.T));
     out[(2 * m) * p.out_sn] = 2 * (dst ? a.y : a.x);
     out[(N - 1 - 2 * m) * p.out_sn] = 2 * (dst ? b.y : b.x);
   }

@@ -232,10 +232,24 @@ __device__ __forceinline__ void big_pass(const Params& mp, const cpx* src, cpx* 
   }
 }
 
+// A line step over one long item by the whole CTA: each thread takes items
+// tid, tid + blockDim.x, ... and issues the loads of kBatch of them before
+// computing and storing any, so the CTA keeps several loads per thread in
+// flight instead of one (this walk is a single CTA's, not a grid's).
 template <class Op>
 __device__ __forceinline__ void cta_line(const LineParams& lp) {
+  constexpr int kBatch = sizeof(typename Op::In) <= 3 * sizeof(cpx) ? 4 : 2;
   const int64_t total = Op::count(lp);
-  for (int64_t e = threadIdx.x; e < total; e += blockDim.x) Op::item(lp, e);
+  const int64_t step = blockDim.x;
+  int64_t e = threadIdx.x;
+  for (; e + (kBatch - 1) * step < total; e += kBatch * step) {
+    typename Op::In v[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) v[u] = Op::load(lp, e + u * step);
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) Op::finish(lp, e + u * step, v[u]);
+  }
+  for (; e < total; e += step) Op::item(lp, e);
 }
 
 template <int LG>
