@@ -1203,6 +1203,103 @@ struct StoreT4Chain {
   }
 };
 
+// Element-wise steps of a long real transform fused into the first or last
+// pass of a Stockham chain whose sub-DFTs hold single points of the
+// half-length sequence (one line, no mirror pairing; the mixed batch's long
+// items).  Point g of sub-DFT b is b1 + n*in_n (first pass, b1 = b % d1),
+// point m of the output is the sub-DFT's normal offset + k*out_k (last
+// pass); N = kn reals in the line.
+
+// Type-2 permutation (Op_dct2_pre): t_g = (u_2g, u_2g+1), u_i = x[2i] for
+// i < N/2, else sg * x[2N-1-2i].
+struct LoadDCT2Chain {
+  static constexpr bool kComplexIn = false;  // whether the raw input elements are complex
+  static constexpr bool kStaged = false;
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+    constexpr int TPT = L / R;
+    const real* in = static_cast<const real*>(p.in);
+    const int64_t N = p.kn, H = N / 2;
+    const real sg = (p.flags & F_DST) ? real(-1) : real(1);
+    const int64_t b1 = umod(x.b, p.d1);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t g = b1 + int64_t(x.j + r * TPT) * p.in_n;
+      const int64_t i0 = 2 * g, i1 = 2 * g + 1;
+      v[r] = cmk(i0 < H ? in[2 * i0] : sg * in[2 * N - 1 - 2 * i0], i1 < H ? in[2 * i1] : sg * in[2 * N - 1 - 2 * i1]);
+    }
+  }
+};
+
+// Type-4 pre-rotation (Op_t4_pre) with a direct root table t1 = w_2N^g.
+struct LoadT4Direct {
+  static constexpr bool kComplexIn = false;  // whether the raw input elements are complex
+  static constexpr bool kStaged = false;
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, cpx (&v)[R]) {
+    constexpr int TPT = L / R;
+    const real* in = static_cast<const real*>(p.in);
+    const int64_t N = p.kn;
+    const bool dst = (p.flags & F_DST) != 0;
+    const int64_t b1 = umod(x.b, p.d1);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t g = b1 + int64_t(x.j + r * TPT) * p.in_n;
+      const real a = in[2 * g], b = in[N - 1 - 2 * g];
+      const cpx w = ldg(p.t1 + g);
+      if (!dst) {
+        v[r] = cmul(w, cmk(a, b));
+      } else {
+        const cpx q = cmul(w, cmk(a, -b));
+        v[r] = cmk(-q.x, -q.y);
+      }
+    }
+  }
+};
+
+// Type-3 de-interleave (Op_dct3_post) of point m of the forward result.
+struct StoreDCT3Chain {
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, const TileOffsets&,
+                                             cpx (&v)[R]) {
+    if (!x.active) return;
+    constexpr int TPT = L / R;
+    real* out = static_cast<real*>(p.out);
+    const int64_t N = p.kn, H = N / 2;
+    const bool dst = (p.flags & F_DST) != 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t m = x.oout + int64_t(x.j + r * TPT) * p.out_k;
+      const cpx w = cconj(v[r]);
+      const int64_t i0 = 2 * m, i1 = 2 * m + 1;
+      out[i0 < H ? 2 * i0 : 2 * N - 1 - 2 * i0] = (dst && i0 >= H) ? -w.x : w.x;
+      out[i1 < H ? 2 * i1 : 2 * N - 1 - 2 * i1] = (dst && i1 >= H) ? -w.y : w.y;
+    }
+  }
+};
+
+// Type-4 post-rotation (Op_t4_post) with a direct root table t2 = w_8N^(2q+1).
+struct StoreT4Direct {
+  template <int L, int R>
+  static __device__ __forceinline__ void run(const AxisParams& p, const Ctx& x, const Tile&, const TileOffsets&,
+                                             cpx (&v)[R]) {
+    if (!x.active) return;
+    constexpr int TPT = L / R;
+    real* out = static_cast<real*>(p.out);
+    const int64_t N = p.kn;
+    const bool dst = (p.flags & F_DST) != 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t m = x.oout + int64_t(x.j + r * TPT) * p.out_k;
+      const cpx T = v[r];
+      const cpx a = cmul(ldg(p.t2 + 2 * m), T);
+      const cpx b = cmul(ldg(p.t2 + (N - 1 - 2 * m)), cconj(T));
+      out[2 * m] = 2 * (dst ? a.y : a.x);
+      out[N - 1 - 2 * m] = 2 * (dst ? b.y : b.x);
+    }
+  }
+};
+
 // The fused type-4 passes take mirror pairs of sub-DFTs into one CTA: with
 // M = d0*d1 sub-DFTs per line, slots c < cpb/2 hold sub-DFTs i of the line
 // and slots c + cpb/2 their mirrors M-1-i (the planner makes cpb even and a

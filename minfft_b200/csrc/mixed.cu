@@ -167,9 +167,14 @@ __device__ __noinline__ void run_small(const Params& mp, const Item& it, unsigne
 
 // One Stockham pass over global memory of a long transform of length 2^LG,
 // sub-DFTs of length RP, span NS (1 or the length of the first pass).
-template <int LG, int RP, int NS>
-__device__ __forceinline__ void big_pass(const Params& mp, const cpx* src, cpx* dst, int flags,
-                                         unsigned char* smem) {
+// Ld / St: the load and store stages (complex by default; the fused type-2
+// permutation and type-4 pre-rotation in the first pass, the fused type-3
+// de-interleave and type-4 post-rotation in the last, with the line's real
+// length kn and direct root tables t1, t2).
+template <int LG, int RP, int NS, class Ld = LoadCplx, class St = StoreCplx>
+__device__ __forceinline__ void big_pass(const Params& mp, const void* src, void* dst, int flags,
+                                         unsigned char* smem, int64_t kn = 0, const cpx* t1 = nullptr,
+                                         const cpx* t2 = nullptr) {
   constexpr int Lc = 1 << LG;
   constexpr int R = 16;
   constexpr int TPT = RP / R;
@@ -202,6 +207,9 @@ __device__ __forceinline__ void big_pass(const Params& mp, const cpx* src, cpx* 
   p.colmode = 1;
   p.flags = flags | (NS == 1 ? F_STAGE_ROWS : 0);
   p.lp = tile_pitch(RP, R, CPB, 1);
+  p.kn = kn;
+  p.t1 = t1;
+  p.t2 = t2;
   int64_t* offs = reinterpret_cast<int64_t*>(smem);
   Tile t{reinterpret_cast<cpx*>(smem + kOffsetsBytes), p.lp};
   const int c = threadIdx.x % CPB, j = threadIdx.x / CPB;
@@ -225,9 +233,9 @@ __device__ __forceinline__ void big_pass(const Params& mp, const cpx* src, cpx* 
     x.oin = offs[c];
     x.oout = offs[CPB + c];
     cpx v[R];
-    LoadCplx::template run<RP, R>(p, x, t, v);
+    Ld::template run<RP, R>(p, x, t, v);
     run_passes<RP, R, 1>(v, j, c, t, p.tw);
-    StoreCplx::template run<RP, R>(p, x, t, to, v);
+    St::template run<RP, R>(p, x, t, to, v);
     __syncthreads();
   }
 }
@@ -269,51 +277,58 @@ __device__ __noinline__ void run_big(const Params& mp, const Item& it, unsigned 
   lp.in_sn = 1;
   lp.out_sn = 1;
   lp.flags = it.flags;
+  const int64_t N = int64_t(1) << log2N;  // the real length (real kinds)
   const cpx* src = static_cast<const cpx*>(job.in);
-  // element-wise pre-processing into S1 (real kinds whose input is not a complex view)
-  if (it.combo == K_C2R || it.combo == K_DCT2 || it.combo == K_DCT3 || it.combo == K_T4) {
+  // element-wise pre-processing into S1 where it needs the pair (k, L-k)
+  // (the type-2 permutation and type-4 pre-rotation are fused into the
+  // first pass instead)
+  if (it.combo == K_C2R || it.combo == K_DCT3) {
     lp.in = job.in;
     lp.out = S1;
     if (it.combo == K_C2R) {
       lp.t2 = mp.rft[log2N];
       cta_line<Op_c2r_pack>(lp);
-    } else if (it.combo == K_DCT2) {
-      cta_line<Op_dct2_pre>(lp);
-    } else if (it.combo == K_DCT3) {
+    } else {
       lp.t1 = mp.t23[log2N];
       lp.t2 = mp.rft[log2N];
       cta_line<Op_dct3_pack>(lp);
-    } else {
-      lp.t1 = mp.t4a[log2N];
-      cta_line<Op_t4_pre>(lp);
     }
     src = S1;
     __syncthreads();
   }
   cpx* mid = (src == S1) ? S2 : S1;
   const bool inv_cplx = (it.combo == K_CPLX) && (it.flags & F_CONJ_IN);
-  big_pass<LG, R1, 1>(mp, src, mid, inv_cplx ? F_CONJ_IN : 0, smem);
+  const int kf = it.flags & F_DST;
+  if (it.combo == K_DCT2)
+    big_pass<LG, R1, 1, LoadDCT2Chain>(mp, job.in, mid, kf, smem, N);
+  else if (it.combo == K_T4)
+    big_pass<LG, R1, 1, LoadT4Direct>(mp, job.in, mid, kf, smem, N, mp.t4a[log2N]);
+  else
+    big_pass<LG, R1, 1>(mp, src, mid, inv_cplx ? F_CONJ_IN : 0, smem);
   __syncthreads();
-  const bool direct = (it.combo == K_CPLX || it.combo == K_C2R);
-  cpx* fin = direct ? static_cast<cpx*>(job.out) : (mid == S1 ? S2 : S1);
+  // the last pass writes the output itself for the complex DFT, the
+  // inverse real DFT and the fused type-3 de-interleave and type-4
+  // post-rotation; the real DFT and the DCT-2 unpack the pairs afterwards
+  const bool pairs = it.combo == K_R2C || it.combo == K_DCT2;
+  cpx* fin = pairs ? (mid == S1 ? S2 : S1) : static_cast<cpx*>(job.out);
   const bool conj_out = inv_cplx || it.combo == K_C2R;
-  big_pass<LG, R2, R1>(mp, mid, fin, conj_out ? F_CONJ_OUT : 0, smem);
+  if (it.combo == K_DCT3)
+    big_pass<LG, R2, R1, LoadCplx, StoreDCT3Chain>(mp, mid, job.out, kf, smem, N);
+  else if (it.combo == K_T4)
+    big_pass<LG, R2, R1, LoadCplx, StoreT4Direct>(mp, mid, job.out, kf, smem, N, nullptr, mp.t4b[log2N]);
+  else
+    big_pass<LG, R2, R1>(mp, mid, fin, conj_out ? F_CONJ_OUT : 0, smem);
   __syncthreads();
-  if (!direct) {
+  if (pairs) {
     lp.in = fin;
     lp.out = job.out;
     if (it.combo == K_R2C) {
       lp.t1 = mp.rft[log2N];
       cta_line<Op_r2c_unpack>(lp);
-    } else if (it.combo == K_DCT2) {
+    } else {
       lp.t1 = mp.t23[log2N];
       lp.t2 = mp.rft[log2N];
       cta_line<Op_dct2_post>(lp);
-    } else if (it.combo == K_DCT3) {
-      cta_line<Op_dct3_post>(lp);
-    } else {
-      lp.t2 = mp.t4b[log2N];
-      cta_line<Op_t4_post>(lp);
     }
   }
 }
