@@ -37,10 +37,10 @@ struct ItemIdx {
 
 __device__ __forceinline__ ItemIdx split_item(int64_t e, int64_t inner, int64_t K) {
   ItemIdx r;
-  const int64_t q = udiv(e, inner);
-  r.i = e - q * inner;
-  r.o = udiv(q, K);
-  r.n = q - r.o * K;
+  r.i = e % inner;
+  const int64_t q = e / inner;
+  r.n = q % K;
+  r.o = q / K;
   return r;
 }
 
@@ -53,23 +53,31 @@ struct Op_dct2_pre {
   struct In {
     real a, b;
   };
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
     const int64_t L = p.L, N = 2 * L;
-    const ItemIdx it = split_item(e, p.inner, L);
     const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
     const int64_t i0 = 2 * it.n, i1 = 2 * it.n + 1;
     return In{i0 < L ? in[(2 * i0) * p.in_sn] : in[(2 * N - 1 - 2 * i0) * p.in_sn],
               i1 < L ? in[(2 * i1) * p.in_sn] : in[(2 * N - 1 - 2 * i1) * p.in_sn]};
   }
-  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& v) {
     const int64_t L = p.L;
     const real sg = (p.flags & F_DST) ? real(-1) : real(1);
-    const ItemIdx it = split_item(e, p.inner, L);
     const int64_t i0 = 2 * it.n, i1 = 2 * it.n + 1;
     static_cast<cpx*>(p.out)[it.o * p.out_so + it.n * p.out_sn + it.i] =
         cmk(i0 < L ? v.a : sg * v.a, i1 < L ? v.b : sg * v.b);
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
+    return split_item(e, p.inner, p.L);
+  }
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    finish_at(p, index(p, e), v);
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const ItemIdx it = index(p, e);
+    finish_at(p, it, load_at(p, it));
+  }
 };
 
 // type-4 pre-rotation (see LoadT4)
@@ -82,15 +90,13 @@ struct Op_t4_pre {
     real a, b;
     cpx w;
   };
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
     const int64_t L = p.L, N = 2 * L;
-    const ItemIdx it = split_item(e, p.inner, L);
     const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
     return In{in[(2 * it.n) * p.in_sn], in[(N - 1 - 2 * it.n) * p.in_sn], root1(p, it.n)};
   }
-  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& x) {
+  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& x) {
     const bool dst = (p.flags & F_DST) != 0;
-    const ItemIdx it = split_item(e, p.inner, p.L);
     cpx v;
     if (!dst) {
       v = cmul(x.w, cmk(x.a, x.b));
@@ -100,7 +106,17 @@ struct Op_t4_pre {
     }
     static_cast<cpx*>(p.out)[it.o * p.out_so + it.n * p.out_sn + it.i] = v;
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
+    return split_item(e, p.inner, p.L);
+  }
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    finish_at(p, index(p, e), v);
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const ItemIdx it = index(p, e);
+    finish_at(p, it, load_at(p, it));
+  }
 };
 
 // inverse-real-DFT packing, conjugated (see LoadC2R); in: L+1 spectrum values
@@ -112,16 +128,14 @@ struct Op_c2r_pack {
   struct In {
     cpx z0, z1, f;
   };
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
     const int64_t L = p.L, K = L / 2 + 1;
-    const ItemIdx it = split_item(e, p.inner, K);
     const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
     const int64_t k = it.n;
     return In{in[k * p.in_sn], in[(L - k) * p.in_sn], (k != 0 && 2 * k != L) ? root2(p, k) : czero()};
   }
-  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& v) {
     const int64_t L = p.L, K = L / 2 + 1;
-    const ItemIdx it = split_item(e, p.inner, K);
     cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
     const int64_t k = it.n;
     if (k == 0) {
@@ -135,7 +149,17 @@ struct Op_c2r_pack {
       out[(L - k) * p.out_sn] = cconj(tb);
     }
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
+    return split_item(e, p.inner, p.L / 2 + 1);
+  }
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    finish_at(p, index(p, e), v);
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const ItemIdx it = index(p, e);
+    finish_at(p, it, load_at(p, it));
+  }
 };
 
 // type-3 pre-rotation + packing, conjugated (see LoadDCT3)
@@ -148,10 +172,9 @@ struct Op_dct3_pack {
     cpx z0, z1, f;
   };
   // the reads and the pre-rotation of both values of the pair
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
     const int64_t L = p.L, K = L / 2 + 1;
     const bool dst = (p.flags & F_DST) != 0;
-    const ItemIdx it = split_item(e, p.inner, K);
     const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
     const int k = int(it.n);
     auto rd = [&](int i) { return in[int64_t(i) * p.in_sn]; };
@@ -159,9 +182,8 @@ struct Op_dct3_pack {
               LoadDCT3::zval_w(rd, int(L) - k, int(L), dst, [&](int n) { return root1(p, n); }),
               (k != 0 && 2 * k != L) ? root2(p, k) : czero()};
   }
-  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& v) {
     const int64_t L = p.L, K = L / 2 + 1;
-    const ItemIdx it = split_item(e, p.inner, K);
     cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
     const int k = int(it.n);
     const cpx z0 = v.z0, z1 = v.z1;
@@ -176,7 +198,17 @@ struct Op_dct3_pack {
       out[(L - k) * p.out_sn] = cconj(tb);
     }
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
+    return split_item(e, p.inner, p.L / 2 + 1);
+  }
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    finish_at(p, index(p, e), v);
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const ItemIdx it = index(p, e);
+    finish_at(p, it, load_at(p, it));
+  }
 };
 
 // real-DFT unpacking (see StoreR2C); out: L+1 spectrum values
@@ -188,17 +220,15 @@ struct Op_r2c_unpack {
   struct In {
     cpx za, zb, f;
   };
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
     const int64_t L = p.L, K = L / 2 + 1;
-    const ItemIdx it = split_item(e, p.inner, K);
     const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
     const int64_t k = it.n;
     const bool pair = k != 0 && 2 * k != L;
     return In{in[k * p.in_sn], pair ? in[(L - k) * p.in_sn] : czero(), pair ? root1(p, k) : czero()};
   }
-  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& v) {
     const int64_t L = p.L, K = L / 2 + 1;
-    const ItemIdx it = split_item(e, p.inner, K);
     cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
     const int64_t k = it.n;
     const cpx za = v.za;
@@ -214,7 +244,17 @@ struct Op_r2c_unpack {
       out[(L - k) * p.out_sn] = xb;
     }
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
+    return split_item(e, p.inner, p.L / 2 + 1);
+  }
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    finish_at(p, index(p, e), v);
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const ItemIdx it = index(p, e);
+    finish_at(p, it, load_at(p, it));
+  }
 };
 
 // type-2 unpacking + post-rotation (see StoreDCT2)
@@ -226,21 +266,19 @@ struct Op_dct2_post {
   struct In {
     cpx za, zb, f, ea, eb;
   };
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
     const int64_t L = p.L, K = L / 2 + 1;
-    const ItemIdx it = split_item(e, p.inner, K);
     const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
     const int64_t k = it.n;
     const bool pair = k != 0 && 2 * k != L;
     return In{in[k * p.in_sn], pair ? in[(L - k) * p.in_sn] : czero(), pair ? root2(p, k) : czero(),
               k != 0 ? root1(p, k) : czero(), pair ? root1(p, L - k) : czero()};
   }
-  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& v) {
     const int64_t L = p.L, K = L / 2 + 1;
     const int N = int(2 * L);
     const bool dst = (p.flags & F_DST) != 0;
     const real r2 = real(1.414213562373095048801688724209698079);
-    const ItemIdx it = split_item(e, p.inner, K);
     real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
     const int k = int(it.n);
     const cpx za = v.za;
@@ -257,7 +295,17 @@ struct Op_dct2_post {
       StoreDCT2::emit2(out, p.out_sn, int(L) - k, N, dst, xb, v.eb);
     }
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
+    return split_item(e, p.inner, p.L / 2 + 1);
+  }
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
+  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    finish_at(p, index(p, e), v);
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const ItemIdx it = index(p, e);
+    finish_at(p, it, load_at(p, it));
+  }
 };
 
 // type-3 de-interleave of the conjugated forward result (see StoreDCT3)
@@ -269,15 +317,23 @@ struct Op_dct3_post {
   struct In {
     cpx w;
   };
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
-    const ItemIdx it = split_item(e, p.inner, p.L);
+  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
     return In{static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i]};
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
+    return split_item(e, p.inner, p.L);
+  }
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
   static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    finish_at(p, index(p, e), v);
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const ItemIdx it = index(p, e);
+    finish_at(p, it, load_at(p, it));
+  }
+  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& v) {
     const int64_t L = p.L, N = 2 * L;
     const bool dst = (p.flags & F_DST) != 0;
-    const ItemIdx it = split_item(e, p.inner, L);
     const cpx w = cconj(v.w);
     real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
     const int64_t i0 = 2 * it.n, i1 = 2 * it.n + 1;
@@ -297,18 +353,26 @@ struct Op_t4_post {
   struct In {
     cpx T, ga, gb;
   };
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) {
+  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
     const int64_t N = 2 * p.L;
-    const ItemIdx it = split_item(e, p.inner, p.L);
     const int64_t m = it.n;
     return In{static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i], root2(p, 2 * m),
               root2(p, N - 1 - 2 * m)};
   }
-  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) { finish(p, e, load(p, e)); }
+  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
+    return split_item(e, p.inner, p.L);
+  }
+  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
   static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
+    finish_at(p, index(p, e), v);
+  }
+  static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
+    const ItemIdx it = index(p, e);
+    finish_at(p, it, load_at(p, it));
+  }
+  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& v) {
     const int64_t L = p.L, N = 2 * L;
     const bool dst = (p.flags & F_DST) != 0;
-    const ItemIdx it = split_item(e, p.inner, L);
     real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
     const int64_t m = it.n;
     const cpx a = cmul(v.ga, v.T);

@@ -14,9 +14,10 @@
 // atomic counter until the list is exhausted.  Short items run the same
 // load -> Stockham passes -> store code as the axis passes, with each
 // transform's own input and output pointers.  Long items (2^14 .. 2^16
-// complex points) run by default on one CTA each: the element-wise
-// pre-processing, two Stockham passes over global memory through the CTA's
-// private scratch slice and the post-processing.  With
+// complex points) run by default on one CTA each: two Stockham passes over
+// global memory through the CTA's private scratch slice, with the kind's
+// element-wise steps fused into them where they need no (k, L-k) pairing
+// and run as sweeps of the CTA before or after them otherwise.  With
 // MINFFT_B200_MIXED_CLUSTER=1 (where the device can co-schedule the clusters)
 // they run instead on clusters of eight CTAs entirely in distributed shared
 // memory (mixed_cluster_kernel, run_cluster_big): the clusters take the long
@@ -249,15 +250,16 @@ __device__ __forceinline__ void cta_line(const LineParams& lp) {
   constexpr int kBatch = sizeof(typename Op::In) <= 3 * sizeof(cpx) ? 4 : 2;
   const int64_t total = Op::count(lp);
   const int64_t step = blockDim.x;
+  // one line (outer = inner = 1): item e is point e of the line
   int64_t e = threadIdx.x;
   for (; e + (kBatch - 1) * step < total; e += kBatch * step) {
     typename Op::In v[kBatch];
 #pragma unroll
-    for (int u = 0; u < kBatch; ++u) v[u] = Op::load(lp, e + u * step);
+    for (int u = 0; u < kBatch; ++u) v[u] = Op::load_at(lp, ItemIdx{0, e + u * step, 0});
 #pragma unroll
-    for (int u = 0; u < kBatch; ++u) Op::finish(lp, e + u * step, v[u]);
+    for (int u = 0; u < kBatch; ++u) Op::finish_at(lp, ItemIdx{0, e + u * step, 0}, v[u]);
   }
-  for (; e < total; e += step) Op::item(lp, e);
+  for (; e < total; e += step) Op::finish_at(lp, ItemIdx{0, e, 0}, Op::load_at(lp, ItemIdx{0, e, 0}));
 }
 
 template <int LG>
