@@ -1,10 +1,10 @@
 // Element-wise pre- and post-processing steps of real-data transforms whose
 // half-length complex DFT runs as several HBM passes, and the length-1 axis
 // steps, as device functions: Op::count(p) work items, Op::item(p, e) does
-// item e.  The steps of the real kinds also come as Op::load(p, e), which
-// reads everything item e needs (data and roots) into an Op::In, and
-// Op::finish(p, e, in), which computes and stores: a CTA that walks a line
-// alone (the mixed-batch kernel) then issues the loads of several items
+// item e.  The steps the mixed-batch kernel runs as sweeps also come as
+// Op::load_at(p, it), which reads everything item it needs (data and roots)
+// into an Op::In, and Op::finish_at(p, it, in), which computes and stores:
+// a CTA that walks a line alone then issues the loads of several items
 // before any of their stores.  Used by the line kernels (line_kernels.cu)
 // and by the mixed-batch kernel (mixed.cu).
 //
@@ -80,42 +80,47 @@ struct Op_dct2_pre {
   }
 };
 
-// type-4 pre-rotation (see LoadT4)
+// The type-4 steps take each point n < L/2 with its mirror n' = L-1-n:
+// x[2n+1] = x[N-1-2n'] and x[N-2-2n] = x[2n'], so the pair reads the reals
+// (x[2n], x[2n+1]) and (x[N-2-2n], x[N-1-2n]), and the post-rotation writes
+// (y[2m], y[2m+1]) and (y[N-2-2m], y[N-1-2m]), as vectors where a line is
+// contiguous and aligned (whole sectors instead of single reals at a
+// stride of two).
+template <class T>
+__device__ __forceinline__ bool pair_vec(const T* base, const LineParams& p, int64_t sn) {
+  return sn == 1 && p.inner == 1 && (reinterpret_cast<uintptr_t>(base) % sizeof(cpx)) == 0;
+}
+
+// type-4 pre-rotation (see LoadT4), points n and L-1-n per item
 struct Op_t4_pre {
-  static __device__ __forceinline__ int64_t count(const LineParams& p) {
-    const int64_t L = p.L;
-    return p.outer * p.inner * L;
-  }
-  struct In {
-    real a, b;
-    cpx w;
-  };
-  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
-    const int64_t L = p.L, N = 2 * L;
-    const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
-    return In{in[(2 * it.n) * p.in_sn], in[(N - 1 - 2 * it.n) * p.in_sn], root1(p, it.n)};
-  }
-  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& x) {
-    const bool dst = (p.flags & F_DST) != 0;
-    cpx v;
-    if (!dst) {
-      v = cmul(x.w, cmk(x.a, x.b));
-    } else {
-      const cpx q = cmul(x.w, cmk(x.a, -x.b));
-      v = cmk(-q.x, -q.y);
-    }
-    static_cast<cpx*>(p.out)[it.o * p.out_so + it.n * p.out_sn + it.i] = v;
-  }
-  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
-    return split_item(e, p.inner, p.L);
-  }
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
-  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
-    finish_at(p, index(p, e), v);
+  static __device__ __forceinline__ int64_t count(const LineParams& p) { return p.outer * p.inner * (p.L / 2); }
+  static __device__ __forceinline__ cpx rot(bool dst, cpx w, real a, real b) {
+    if (!dst) return cmul(w, cmk(a, b));
+    const cpx q = cmul(w, cmk(a, -b));
+    return cmk(-q.x, -q.y);
   }
   static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
-    const ItemIdx it = index(p, e);
-    finish_at(p, it, load_at(p, it));
+    const int64_t L = p.L, N = 2 * L;
+    const bool dst = (p.flags & F_DST) != 0;
+    const ItemIdx it = split_item(e, p.inner, L / 2);
+    const int64_t n = it.n, m = L - 1 - n, sn = p.in_sn;
+    const real* in = static_cast<const real*>(p.in) + it.o * p.in_so + it.i;
+    real x0, x1, y0, y1;  // x[2n], x[2n+1], x[N-2-2n], x[N-1-2n]
+    if (pair_vec(in, p, sn)) {
+      const cpx u = *reinterpret_cast<const cpx*>(in + 2 * n), w = *reinterpret_cast<const cpx*>(in + N - 2 - 2 * n);
+      x0 = u.x;
+      x1 = u.y;
+      y0 = w.x;
+      y1 = w.y;
+    } else {
+      x0 = in[(2 * n) * sn];
+      x1 = in[(2 * n + 1) * sn];
+      y0 = in[(N - 2 - 2 * n) * sn];
+      y1 = in[(N - 1 - 2 * n) * sn];
+    }
+    cpx* out = static_cast<cpx*>(p.out) + it.o * p.out_so + it.i;
+    out[n * p.out_sn] = rot(dst, root1(p, n), x0, y1);
+    out[m * p.out_sn] = rot(dst, root1(p, m), y0, x1);
   }
 };
 
@@ -344,41 +349,34 @@ struct Op_dct3_post {
   }
 };
 
-// type-4 post-rotation (see StoreT4)
+// type-4 post-rotation (see StoreT4), points m and L-1-m per item
 struct Op_t4_post {
-  static __device__ __forceinline__ int64_t count(const LineParams& p) {
-    const int64_t L = p.L;
-    return p.outer * p.inner * L;
-  }
-  struct In {
-    cpx T, ga, gb;
-  };
-  static __device__ __forceinline__ In load_at(const LineParams& p, const ItemIdx& it) {
-    const int64_t N = 2 * p.L;
-    const int64_t m = it.n;
-    return In{static_cast<const cpx*>(p.in)[it.o * p.in_so + it.n * p.in_sn + it.i], root2(p, 2 * m),
-              root2(p, N - 1 - 2 * m)};
-  }
-  static __device__ __forceinline__ ItemIdx index(const LineParams& p, int64_t e) {
-    return split_item(e, p.inner, p.L);
-  }
-  static __device__ __forceinline__ In load(const LineParams& p, int64_t e) { return load_at(p, index(p, e)); }
-  static __device__ __forceinline__ void finish(const LineParams& p, int64_t e, const In& v) {
-    finish_at(p, index(p, e), v);
-  }
+  static __device__ __forceinline__ int64_t count(const LineParams& p) { return p.outer * p.inner * (p.L / 2); }
   static __device__ __forceinline__ void item(const LineParams& p, int64_t e) {
-    const ItemIdx it = index(p, e);
-    finish_at(p, it, load_at(p, it));
-  }
-  static __device__ __forceinline__ void finish_at(const LineParams& p, const ItemIdx& it, const In& v) {
     const int64_t L = p.L, N = 2 * L;
     const bool dst = (p.flags & F_DST) != 0;
+    const ItemIdx it = split_item(e, p.inner, L / 2);
+    const int64_t m = it.n, mm = L - 1 - m;
+    const cpx* in = static_cast<const cpx*>(p.in) + it.o * p.in_so + it.i;
+    const cpx T = in[m * p.in_sn], U = in[mm * p.in_sn];
+    // y[2m] = 2 Re(g_2m T_m), y[N-1-2m] = 2 Re(g_(N-1-2m) conj(T_m)); the
+    // mirror's y[2mm] = y[N-2-2m] and y[N-1-2mm] = y[2m+1] (Im for DST-4)
+    auto part = [&](cpx v) { return 2 * (dst ? v.y : v.x); };
+    const real a0 = part(cmul(root2(p, 2 * m), T));            // y[2m]
+    const real b0 = part(cmul(root2(p, N - 1 - 2 * m), cconj(T)));  // y[N-1-2m]
+    const real a1 = part(cmul(root2(p, N - 2 - 2 * m), U));    // y[N-2-2m]
+    const real b1 = part(cmul(root2(p, 2 * m + 1), cconj(U)));  // y[2m+1]
     real* out = static_cast<real*>(p.out) + it.o * p.out_so + it.i;
-    const int64_t m = it.n;
-    const cpx a = cmul(v.ga, v.T);
-    const cpx b = cmul(v.gb, cconj(v.T));
-    out[(2 * m) * p.out_sn] = 2 * (dst ? a.y : a.x);
-    out[(N - 1 - 2 * m) * p.out_sn] = 2 * (dst ? b.y : b.x);
+    const int64_t sn = p.out_sn;
+    if (pair_vec(out, p, sn)) {
+      *reinterpret_cast<cpx*>(out + 2 * m) = cmk(a0, b1);
+      *reinterpret_cast<cpx*>(out + N - 2 - 2 * m) = cmk(a1, b0);
+    } else {
+      out[(2 * m) * sn] = a0;
+      out[(2 * m + 1) * sn] = b1;
+      out[(N - 2 - 2 * m) * sn] = a1;
+      out[(N - 1 - 2 * m) * sn] = b0;
+    }
   }
 };
 

@@ -1551,6 +1551,7 @@ struct Planner {
       } else if (s.combo == mb::K_T4) {
         which = mb::LK_T4_PRE;
         set_root_pair(lp, 1, 2 * s.N, 1, 0);  // w_2N^n
+        items = outer * inner * (Lt / 2);      // points n and Lt-1-n per item
       } else if (s.combo == mb::K_C2R) {
         which = mb::LK_C2R_PACK;
         set_root_pair(lp, 2, s.N, 1, 0);  // w_N^k
@@ -1657,7 +1658,7 @@ struct Planner {
       } else {
         which = mb::LK_T4_POST;
         set_root_pair(lp, 2, 8 * s.N, 2, 1);  // w_8N^(2q+1)
-        items = outer * inner * Lt;
+        items = outer * inner * (Lt / 2);      // points m and Lt-1-m per item
       }
       add_line_kernel(which, lp, items, cd, s.out_buf);
     }
