@@ -1533,13 +1533,21 @@ struct Planner {
       lp.flags = s.flags;
       return lp;
     };
-    // A 1-D type-4 chain of two or more passes in FP32 fuses its pre-rotation
-    // into the first pass's load and its post-rotation into the last pass's
-    // store (LoadT4Chain, StoreT4Chain): two passes over HBM instead of four.
+    // A 1-D type-4 chain of two or more passes fuses its pre-rotation into
+    // the first pass's load and its post-rotation into the last pass's store
+    // (LoadT4Chain, StoreT4Chain): two passes over HBM instead of four.  In a
+    // tensor-core mode only an end pass on the CUDA cores fuses its rotation
+    // (the 256-point tensor-core passes take plain complex input and output);
+    // the other rotation stays a separate element-wise step.
     // (the fused passes form their roots from 32-bit exponents into the tables of 8N)
-    const bool t4_fused = s.combo == mb::K_T4 && inner == 1 && P >= 2 && a->precision == MINFFT_B200_PREC_FP32 &&
-                          s.N <= (int64_t(1) << 28) && t4_fuse_enabled();
-    if (!t4_fused &&
+    const bool t4_chain =
+        s.combo == mb::K_T4 && inner == 1 && P >= 2 && s.N <= (int64_t(1) << 28) && t4_fuse_enabled();
+    auto cuda_core_pass = [&](int p) {
+      return a->precision == MINFFT_B200_PREC_FP32 || (int64_t(1) << pb[p]) != mb::kTcLength;
+    };
+    const bool t4_fused_in = t4_chain && cuda_core_pass(0);
+    const bool t4_fused_out = t4_chain && cuda_core_pass(P - 1);
+    if (!t4_fused_in &&
         (s.combo == mb::K_DCT2 || s.combo == mb::K_T4 || s.combo == mb::K_C2R || s.combo == mb::K_DCT3)) {
       cs = BUF_T2;
       need(cs, work_bytes);
@@ -1564,8 +1572,8 @@ struct Planner {
       }
       add_line_kernel(which, lp, items, s.in_buf, cs);
     }
-    const bool post =
-        !t4_fused && (s.combo == mb::K_R2C || s.combo == mb::K_DCT2 || s.combo == mb::K_DCT3 || s.combo == mb::K_T4);
+    const bool post = !t4_fused_out &&
+                      (s.combo == mb::K_R2C || s.combo == mb::K_DCT2 || s.combo == mb::K_DCT3 || s.combo == mb::K_T4);
 
     // --- the HBM passes
     int prev = cs;
@@ -1585,7 +1593,7 @@ struct Planner {
       } else {
         dst = s.out_buf;
       }
-      const bool fuse_in = t4_fused && p == 0, fuse_out = t4_fused && last;
+      const bool fuse_in = t4_fused_in && p == 0, fuse_out = t4_fused_out && last;
       const int64_t Nsp = Ns * inner;
       AxisParams ap = base_params();
       ap.d0 = Nsp;

@@ -231,8 +231,13 @@ def test_tuning_table_file_round_trip(single):
 @pytest.mark.parametrize("precision", ["tc_f16", "tc_bf16"])
 def test_tensor_core_type4_chain(precision):
     """The half-length chain of a 2^24-point DCT-4 (2^23 points) runs two
-    256-point tensor-core passes in a tensor-core mode."""
+    256-point tensor-core passes in a tensor-core mode; the last pass, on the
+    CUDA cores, takes the post-rotation into its store, and the pre-rotation
+    stays a separate element-wise step before the tensor-core pass."""
     eng = minfft_b200.engine(True)
     bad, rep, _ = eng.plan_selfcheck("dct4", (1 << 24,), 1, False, precision=precision)
     assert bad == 0, rep
-    assert chain_passes(rep) == ["tc:256", "tc:256", "cplx:128"], rep
+    assert chain_passes(rep) == ["tc:256", "tc:256", "cplx+t4post:128"], rep
+    labs = rep.splitlines()
+    assert any("line<t4_pre>" in lab for lab in labs), rep
+    assert not any("line<t4_post>" in lab for lab in labs), rep
