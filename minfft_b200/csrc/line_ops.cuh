@@ -35,12 +35,27 @@ struct ItemIdx {
   int64_t o, n, i;
 };
 
+// Item e = (o * K + n) * inner + i.  Power-of-two extents (inner always, K
+// unless it counts L/2+1 spectrum points) split by masks and shifts: the
+// 64-bit quotient sequences otherwise keep the conversion pipe busy for most
+// of a line kernel's time.
 __device__ __forceinline__ ItemIdx split_item(int64_t e, int64_t inner, int64_t K) {
   ItemIdx r;
-  r.i = e % inner;
-  const int64_t q = e / inner;
-  r.n = q % K;
-  r.o = q / K;
+  int64_t q;
+  if ((inner & (inner - 1)) == 0) {
+    r.i = e & (inner - 1);
+    q = e >> (__ffsll(inner) - 1);
+  } else {
+    r.i = e % inner;
+    q = e / inner;
+  }
+  if ((K & (K - 1)) == 0) {
+    r.n = q & (K - 1);
+    r.o = q >> (__ffsll(K) - 1);
+  } else {
+    r.n = q % K;
+    r.o = q / K;
+  }
   return r;
 }
 
