@@ -565,7 +565,7 @@ struct TcsLayout {
   static constexpr int NT = FMT == TC_F16 ? 2 : 3;
   static constexpr int bar_bytes = 128;                  // mbarriers, TMEM slot, flag
   static constexpr int b_off = bar_bytes;                // B operands: NT x 2 KB
-  static constexpr int tw_off = b_off + NT * kBBytes;    // w_256^m, m < 256 (2 KB)
+  static constexpr int tw_off = b_off + NT * kBBytes;    // w_256^(d k1) at 16 k1 + d (2 KB)
   static constexpr int a_off = tw_off + kL * 8;          // A operands: groups x NT x 8 KB
   static constexpr int st_off = a_off + kTcsG * NT * kOpBytes;
   static constexpr int tmem_cols = 64 * kTcsG;           // groups x (leading, correction) x 32
@@ -718,7 +718,10 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 4 : 3) tc_stream_kerne
     const uint4* src = reinterpret_cast<const uint4*>(q.bmat);
     uint4* dst = reinterpret_cast<uint4*>(bop);
     for (int i = tid; i < NT * kBBytes / 16; i += kTcsNT) dst[i] = src[i];
-    for (int i = tid; i < kL; i += kTcsNT) tws[i] = ldg(p.tw + i);  // the twiddles between the stages
+    // the twiddles between the stages, w_256^(d k1) at k1 * 16 + d: the 16
+    // values of d a warp reads for one k1 sit in 16 consecutive slots (no
+    // bank conflicts, where reading w_256^m at m = d k1 put up to 8 in one bank)
+    for (int i = tid; i < kL; i += kTcsNT) tws[i] = ldg(p.tw + (i >> 4) * (i & 15));
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -853,7 +856,7 @@ __global__ void __launch_bounds__(kTcsNT, FMT == TC_F16 ? 4 : 3) tc_stream_kerne
     // unscale and twiddle: y1[k1][n2] * w_256^(n2 k1), n2 = d; into the stage
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) {
-      const cpx w = tws[d * k1];
+      const cpx w = tws[16 * k1 + d];
       const cpx y = cmul(cmk(re[k1] * inv, im[k1] * inv), w);
       const int idx = ROWS ? c * kL + 16 * k1 + (d ^ k1) : (16 * k1 + (d ^ (k1 & 1))) * W + c;
       tile[idx] = y;
