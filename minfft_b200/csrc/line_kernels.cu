@@ -2,16 +2,32 @@
 // half-length complex DFT is too long for one CTA (it then runs as several
 // HBM passes, see plan.cu), plus the length-1 axis kernels.  The element-wise
 // steps themselves are in line_ops.cuh.
+#include <type_traits>
+
 #include "line_ops.cuh"
 
 namespace mb {
 
 namespace {
 
+template <class Op, class = void>
+struct HasItem32 : std::false_type {};
+template <class Op>
+struct HasItem32<Op, std::void_t<decltype(&Op::item32)>> : std::true_type {};
+
+// Grid-stride walk over the items; steps with a 32-bit form (Op::item32)
+// take it when Op::fast(p) holds for the whole launch.
 template <class Op>
 __global__ void k_line(const LineParams p) {
   pdl_release();
   pdl_wait();
+  if constexpr (HasItem32<Op>::value) {
+    if (Op::fast(p)) {
+      const uint32_t total = Op::count32(p), stride = gridDim.x * blockDim.x;
+      for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) Op::item32(p, e);
+      return;
+    }
+  }
   const int64_t total = Op::count(p);
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
     Op::item(p, e);

@@ -137,6 +137,28 @@ struct Op_t4_pre {
     out[n * p.out_sn] = rot(dst, root1(p, n), x0, y1);
     out[m * p.out_sn] = rot(dst, root1(p, m), y0, x1);
   }
+  // One contiguous line (unit strides, an input aligned for the vector
+  // reads) shorter than 2^30 points, with roots w_2N^n: the same item in
+  // 32-bit index arithmetic (the 64-bit products and shifts of the general
+  // form are most of its instructions).
+  static __device__ __forceinline__ bool fast(const LineParams& p) {
+    return p.outer == 1 && p.inner == 1 && p.in_sn == 1 && p.out_sn == 1 && p.hi1 && p.mul1 == 1 &&
+           p.add1 == 0 && p.L < (int64_t(1) << 30) && (reinterpret_cast<uintptr_t>(p.in) % sizeof(cpx)) == 0;
+  }
+  static __device__ __forceinline__ uint32_t count32(const LineParams& p) { return uint32_t(p.L / 2); }
+  static __device__ __forceinline__ void item32(const LineParams& p, uint32_t n) {
+    const uint32_t L = uint32_t(p.L), N = 2 * L, m = L - 1 - n;
+    const real* in = static_cast<const real*>(p.in);
+    const cpx u = *reinterpret_cast<const cpx*>(in + 2 * n);            // x[2n], x[2n+1]
+    const cpx w = *reinterpret_cast<const cpx*>(in + (N - 2 - 2 * n));  // x[N-2-2n], x[N-1-2n]
+    const uint32_t mask = (1u << p.bits1) - 1;
+    const cpx r0 = cmul(ldg(p.hi1 + (n >> p.bits1)), ldg(p.lo1 + (n & mask)));
+    const cpx r1 = cmul(ldg(p.hi1 + (m >> p.bits1)), ldg(p.lo1 + (m & mask)));
+    const bool dst = (p.flags & F_DST) != 0;
+    cpx* out = static_cast<cpx*>(p.out);
+    out[n] = rot(dst, r0, u.x, w.y);
+    out[m] = rot(dst, r1, w.x, u.y);
+  }
 };
 
 // inverse-real-DFT packing, conjugated (see LoadC2R); in: L+1 spectrum values
