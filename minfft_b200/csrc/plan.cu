@@ -1536,14 +1536,16 @@ struct Planner {
     // A 1-D type-4 chain of two or more passes fuses its pre-rotation into
     // the first pass's load and its post-rotation into the last pass's store
     // (LoadT4Chain, StoreT4Chain): two passes over HBM instead of four.  In a
-    // tensor-core mode only an end pass on the CUDA cores fuses its rotation
-    // (the 256-point tensor-core passes take plain complex input and output);
-    // the other rotation stays a separate element-wise step.
+    // tensor-core mode only an end pass on the CUDA cores of 128 to 1024
+    // points (the lengths the FP32 and FP64 type-4 chains take) fuses its
+    // rotation: the 256-point tensor-core passes take plain complex input and
+    // output.  The other rotation stays a separate element-wise step.
     // (the fused passes form their roots from 32-bit exponents into the tables of 8N)
     const bool t4_chain =
         s.combo == mb::K_T4 && inner == 1 && P >= 2 && s.N <= (int64_t(1) << 28) && t4_fuse_enabled();
     auto cuda_core_pass = [&](int p) {
-      return a->precision == MINFFT_B200_PREC_FP32 || (int64_t(1) << pb[p]) != mb::kTcLength;
+      return a->precision == MINFFT_B200_PREC_FP32 ||
+             ((int64_t(1) << pb[p]) != mb::kTcLength && pb[p] >= 7 && pb[p] <= kPassCapLog2Cc);
     };
     const bool t4_fused_in = t4_chain && cuda_core_pass(0);
     const bool t4_fused_out = t4_chain && cuda_core_pass(P - 1);

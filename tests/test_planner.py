@@ -241,3 +241,10 @@ def test_tensor_core_type4_chain(precision):
     labs = rep.splitlines()
     assert any("line<t4_pre>" in lab for lab in labs), rep
     assert not any("line<t4_post>" in lab for lab in labs), rep
+    # a last pass longer than 1024 points (2^19 = 256 x 2048) keeps the
+    # post-rotation as an element-wise step
+    bad, rep, _ = eng.plan_selfcheck("dct4", (1 << 20,), 1, False, precision=precision)
+    assert bad == 0, rep
+    assert chain_passes(rep) == ["tc:256", "cplx:2048"], rep
+    labs = rep.splitlines()
+    assert any("line<t4_pre>" in lab for lab in labs) and any("line<t4_post>" in lab for lab in labs), rep
