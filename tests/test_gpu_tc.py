@@ -166,6 +166,56 @@ def run_rows(op, x, mode):
         plan.free()
 
 
+# (points, post-rotation as a separate element-wise step): the half-length
+# chains 256 x 128 and 256 x 512 end in a CUDA-core pass that takes the
+# post-rotation into its store; 256 x 256 ends on the tensor cores and
+# 256 x 2048 in a pass longer than 1024 points, so both keep the step.
+T4_CHAINS = [(1 << 16, False), (1 << 17, True), (1 << 18, False), (1 << 20, True)]
+
+
+def run_t4(op, x, mode):
+    """One DCT-4 / DST-4 line of x in a TC mode; also the kernel labels of
+    one call (launch-level timing, on a zero input)."""
+    eng = minfft_b200.engine(True)
+    n = x.size
+    plan = eng.plan("t4", (n,))
+    try:
+        eng.set_precision(plan.aux, mode)
+        z = torch.zeros(n, dtype=torch.float32, device="cuda")
+        zo = torch.zeros_like(z)
+        eng.profile(plan.aux, 1)
+        plan(op, z.data_ptr(), zo.data_ptr())
+        labs = [s[0] for s in eng.profile_stats(plan.aux)]
+        eng.profile(plan.aux, 0)
+        xt = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+        y = torch.full((n,), float("nan"), dtype=torch.float32, device="cuda")
+        plan(op, xt.data_ptr(), y.data_ptr())
+        torch.cuda.synchronize()
+        eng.tc_status(plan.aux)
+        return y.cpu().numpy(), labs
+    finally:
+        plan.free()
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("n,line_post", T4_CHAINS, ids=[f"2^{n.bit_length() - 1}" for n, _ in T4_CHAINS])
+def test_tc_type4_chains(n, line_post, mode):
+    """DCT-4 / DST-4 lines whose half-length DFT is a Stockham chain with
+    tensor-core passes: the pre-rotation as an element-wise step (paired
+    points n, L-1-n), the post-rotation fused into a last CUDA-core pass of
+    128 to 1024 points, or else an element-wise step after the chain."""
+    rng = np.random.default_rng(n)
+    x = rng.uniform(-1, 1, n).astype(np.float32)
+    for op in ("dct4", "dst4"):
+        got, labs = run_t4(op, x, mode)
+        assert any(("tc_stream<" in lab or "tc_pass<" in lab) for lab in labs), labs
+        assert any("line<t4_pre>" in lab for lab in labs), labs
+        assert any("line<t4_post>" in lab for lab in labs) == line_post, labs
+        want = oracle.apply(op, x.astype(np.float64), (n,), single=False, kind=oracle.best_kind())
+        err = rel_l2(got, want)
+        assert err <= TC_BAR, (op, n, mode, err)
+
+
 @pytest.mark.parametrize("mode", MODES)
 def test_tc_wide_dynamic_range(mode):
     """Per-row block scaling keeps every transform of a batch accurate when
