@@ -248,3 +248,20 @@ def test_tensor_core_type4_chain(precision):
     assert chain_passes(rep) == ["tc:256", "cplx:2048"], rep
     labs = rep.splitlines()
     assert any("line<t4_pre>" in lab for lab in labs) and any("line<t4_post>" in lab for lab in labs), rep
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tc_f16", "tc_bf16"])
+def test_fused_type4_pass_lengths(precision):
+    """Every 1-D type-4 chain, in every precision mode, fuses its rotations
+    only into passes of 128 to 1024 points, and each rotation is done exactly
+    once: fused into an end pass or as its element-wise step."""
+    eng = minfft_b200.engine(True)
+    for b in range(13, 28):
+        bad, rep, _ = eng.plan_selfcheck("dct4", (1 << b,), 1, False, precision=precision)
+        assert bad == 0, rep
+        fused = re.findall(r"(t4pre\+cplx|cplx\+t4post),L=(\d+)", rep)
+        assert all(128 <= int(L) <= 1024 for _, L in fused), (b, rep)
+        kinds = [k for k, _ in fused]
+        if "line<" in rep or kinds:  # a chain (shorter lines run in one CTA)
+            assert kinds.count("t4pre+cplx") + rep.count("line<t4_pre>") == 1, (b, rep)
+            assert kinds.count("cplx+t4post") + rep.count("line<t4_post>") == 1, (b, rep)
